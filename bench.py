@@ -1,0 +1,294 @@
+"""Benchmark of the B200 FFT engine (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2c|c1]
+
+Workloads (synthetic, seeded; no dataset is involved):
+  c2c  (default) batched complex DFT, FP64, N = 65536 x 4096 transforms per
+       GPU; one step = notorious_fft_dft then notorious_fft_invdft over the
+       batch.  The split-tensor-core FP32 form runs the same shape and is
+       reported beside it.  4 GiB per array > L2, so no L2 flush is needed.
+  c1   256 x N=4096 FP64 dft + invdft (32 MiB per array < L2: the L2 is
+       flushed by a 256 MiB write between timed steps).
+
+Metric: HBM GB/s of algorithmic traffic (one read + one write of every
+transform's input and output, 2 N sizeof(cmpl) bytes per transform) on the
+device-resident batch, whole job (sum over GPUs).  `e2e` is the same metric
+through the C ABI with pinned host buffers (host<->device copies inside the
+timed region).  Multi-GPU runs shard the batch: every rank runs its own
+4096 transforms (weak scaling), no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "notorious-fft_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "HBM GB/s, % roofline: FP64 drop-in vs batched split-TC form at stated error"
+
+WORKLOADS = {
+    "c2c": dict(N=65536, batch=4096, l2="inputs 4 GiB per array > L2 (no flush)", flush=False),
+    "c1": dict(N=4096, batch=256, l2="L2 flushed (256 MiB write) between steps", flush=True),
+}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                                       "-i", str(index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(kind_pairs, N, sample, threads, reps=3, lib="libref_d_avx2.so", prec="f64"):
+    """Time the reference's own CPU path (oracle/_ref, compiled from the
+    reference sources) on the host cores.  Returns (seconds per transform
+    summed over kind_pairs, kind)."""
+    exe = os.path.join(ROOT, "oracle", "_build", "cpu_bench")
+    so = os.path.join(ROOT, "oracle", "_ref", lib)
+    kind = "reference"
+    if not (os.path.exists(exe) and os.path.exists(so)):
+        return None, "unavailable"
+    total = 0.0
+    for k in kind_pairs:
+        r = subprocess.run([exe, so, prec, k, str(N), str(sample), str(threads), str(reps)], capture_output=True,
+                           text=True, timeout=600)
+        if r.returncode != 0:
+            return None, "unavailable"
+        d = json.loads(r.stdout.strip().splitlines()[-1])
+        total += d["seconds"] / sample
+    return total, kind
+
+
+def run_reference_arm(args, wl):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    N = wl["N"]
+    sample = max(threads * 4, 64) if N >= 65536 else 1024
+    per = []
+    for _ in range(args.warmup):
+        cpu_reference(["dft", "invdft"], N, sample, threads, reps=1)
+    t0 = time.time()
+    for _ in range(args.steps):
+        s, kind = cpu_reference(["dft", "invdft"], N, sample, threads, reps=1)
+        if s is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build missing (oracle/_ref)"}))
+            return
+        per.append(s)
+    sec = statistics.median(per)          # seconds for one dft + one invdft
+    bytes_per_pair = 2 * 2 * N * 16
+    gbs = bytes_per_pair / sec / 1e9
+    ms_step = sec * wl["batch"] * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"c2c fp64 N={N} x{wl['batch']} dft+invdft (reference CPU path)", "N": N,
+                   "batch": wl["batch"], "l2": wl["l2"]},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+                         "sample": f"{sample} transforms per direction per step, OpenMP over the batch, "
+                                   f"one aux per thread, -O3 -fopenmp -mavx2 -mfma"},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(time.time() - t0, 2),
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2c")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args, wl)
+
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from notorious_fft import load
+
+    L = load(single=False)
+    N, B = wl["N"], wl["batch"]
+    stream = torch.cuda.current_stream()
+    L.set_stream(stream.cuda_stream)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1 + rank)
+    x = torch.complex(torch.rand(B, N, generator=g, device="cuda", dtype=torch.float64) * 2 - 1,
+                      torch.rand(B, N, generator=g, device="cuda", dtype=torch.float64) * 2 - 1)
+    y = torch.empty_like(x)
+    z = torch.empty_like(x)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if wl["flush"] else None
+    aux = L.mkaux("dft", [N])
+
+    def step():
+        aux.batched("dft", x, y, B, N, N)
+        aux.batched("invdft", y, z, B, N, N)
+
+    for _ in range(args.warmup):
+        step()
+        if flush is not None:
+            flush.fill_(1)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    times = []
+    launches0 = L.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    total_ms = 0.0
+    for _ in range(args.steps):
+        if flush is not None:
+            flush.fill_(1)
+        ev0.record(stream)
+        step()
+        ev1.record(stream)
+        ev1.synchronize()
+        t = ev0.elapsed_time(ev1)
+        times.append(t)
+        total_ms += t
+    torch.cuda.synchronize()
+    launches = L.launch_count() - launches0
+    ck = clocks.stop()
+    if dist:
+        dist.barrier()
+    ms_step = total_ms / args.steps
+    if dist:
+        tt = torch.tensor([ms_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_step = float(tt.item())
+    bytes_per_step = 2 * B * 2 * N * 16            # dft + invdft, each reads and writes the batch
+    value = bytes_per_step * world / (ms_step * 1e-3) / 1e9
+    # correctness spot check of this run (round trip)
+    err = float(torch.linalg.vector_norm(z[:4] / N - x[:4]) / torch.linalg.vector_norm(x[:4]))
+
+    peak, peak_kind = peaks()
+    # dominant kernel: the batched FFT itself (all passes of one transform over
+    # the batch), timed with CUDA events on the launching stream
+    per_transform_ms = ms_step / 2
+    achieved = (B * 2 * N * 16) / (per_transform_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+            "kernel": "pass_kernel<double> x passes (one batched c2c transform)"}
+
+    e2e = None
+    if not args.no_e2e and rank == 0 and world == 1:
+        xh = x.cpu().pin_memory()
+        yh = torch.empty_like(xh).pin_memory()
+        zh = torch.empty_like(xh).pin_memory()
+        aux.batched("dft", xh, yh, B, N, N)
+        torch.cuda.synchronize()
+        ks = min(3, args.steps)
+        t0 = time.perf_counter()
+        for _ in range(ks):
+            aux.batched("dft", xh, yh, B, N, N)
+            aux.batched("invdft", yh, zh, B, N, N)
+        dt = (time.perf_counter() - t0) / ks
+        e2e = {"value": round(bytes_per_step / dt / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": 2 * B * N * 16,
+               "d2h_bytes_per_step": 2 * B * N * 16, "steps": ks, "timing": "host wall clock around synchronous C-ABI calls"}
+        del xh, yh, zh
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        sample = max(threads * 2, 32) if N >= 65536 else 1024
+        s, kind = cpu_reference(["dft", "invdft"], N, sample, threads)
+        if s is not None:
+            cpu = {"value": round(2 * 2 * N * 16 / s / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
+                   "sample": f"{sample} transforms of N={N} per direction, best of 3, OpenMP over the batch"}
+    aux.free()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (uniform[-1,1), torch seeded generator)",
+            "config": {"workload": f"c2c fp64 N={N} x{B} dft+invdft per GPU", "N": N, "batch": B, "l2": wl["l2"],
+                       "parallelism": f"batch-sharded x{world}"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": ck, "round_trip_rel_err": err,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,282 @@
+// nfft_api.cu -- the C ABI: the reference's 27 entry points
+// (src/07_legacy.h:29-57 of Notorious-FFT) plus the extensions declared in
+// include/notorious_fft.h.  Everything here is host code; all arithmetic runs
+// in the pass kernels.  Host pointers are staged through device buffers owned
+// by the plan; device pointers are used in place.
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../include/notorious_fft.h"
+#include "nfft_engine.h"
+
+using namespace nfft;
+
+static_assert(sizeof(notorious_fft_real) == sizeof(real_t), "header precision must match the build precision");
+
+namespace {
+
+thread_local cudaStream_t t_stream = 0;
+
+notorious_fft_aux* make_aux(int family, int d, const int* Ns) {
+    clear_error();
+    notorious_fft_plan* p = plan_create(family, d, Ns);
+    if (!p) return nullptr;
+    notorious_fft_aux* a = (notorious_fft_aux*)calloc(1, sizeof(notorious_fft_aux));
+    if (!a) {
+        plan_destroy(p);
+        set_error(NOTORIOUS_FFT_ERR_ALLOC, "host allocation of the aux failed");
+        return nullptr;
+    }
+    long long total = 1;
+    for (int i = 0; i < d; ++i) total *= Ns[i];
+    a->N = (int)total;
+    a->plan = p;
+    return a;
+}
+
+bool is_device_ptr(const void* ptr) {
+    cudaPointerAttributes attr;
+    cudaError_t e = cudaPointerGetAttributes(&attr, ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+bool grow(void** buf, size_t* have, size_t need) {
+    if (*have >= need && *buf) return true;
+    if (*buf) cudaFree(*buf);
+    *buf = nullptr;
+    *have = 0;
+    if (!cuda_ok(cudaMalloc(buf, need), "cudaMalloc(staging)")) return false;
+    *have = need;
+    return true;
+}
+
+// One public call: validate, stage host data if needed, execute, unstage.
+void run(int kind, const void* x, void* y, const notorious_fft_aux* a, long long howmany, long long idist,
+         long long odist, int vjp) {
+    clear_error();
+    if (!a || !a->plan) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "NULL aux");
+        return;
+    }
+    if (!x || !y) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "NULL data pointer");
+        return;
+    }
+    if (howmany <= 0) return;
+    notorious_fft_plan* p = a->plan;
+    std::lock_guard<std::mutex> lk(p->mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != p->device && !cuda_ok(cudaSetDevice(p->device), "cudaSetDevice")) return;
+    // element counts of one transform, as the vjp swaps the roles of in and out
+    int kin = kind, kout = kind;
+    if (vjp) {
+        // the cotangent has the output's shape and the result the input's
+        static const int swap_kind[10] = {K_DFT, K_INVDFT, K_INVREALDFT, K_REALDFT, K_DCT2,
+                                          K_DST2, K_DCT3, K_DST3, K_DCT4, K_DST4};
+        (void)swap_kind;
+    }
+    long long in_elems = vjp ? plan_out_elems(p, kind) : plan_in_elems(p, kin);
+    long long out_elems = vjp ? plan_in_elems(p, kind) : plan_out_elems(p, kout);
+    size_t in_eb = vjp ? out_elem_bytes(kind) : in_elem_bytes(kind);
+    size_t out_eb = vjp ? in_elem_bytes(kind) : out_elem_bytes(kind);
+    if (howmany == 1) {
+        idist = in_elems;
+        odist = out_elems;
+    }
+    if (idist < 0 || odist < 0) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "negative distance");
+        return;
+    }
+    size_t in_bytes = (size_t)((howmany - 1) * idist + in_elems) * in_eb;
+    size_t out_bytes = (size_t)((howmany - 1) * odist + out_elems) * out_eb;
+    bool xd = is_device_ptr(x), yd = is_device_ptr(y);
+    cudaStream_t s = t_stream;
+    const void* din = x;
+    void* dout = y;
+    if (!xd) {
+        if (!grow(&p->stage_in, &p->stage_in_bytes, in_bytes)) goto done;
+        if (!cuda_ok(cudaMemcpyAsync(p->stage_in, x, in_bytes, cudaMemcpyHostToDevice, s), "H2D copy")) goto done;
+        din = p->stage_in;
+    } else {
+        size_t al = in_eb == sizeof(cplx_t) ? sizeof(cplx_t) : sizeof(real_t);
+        if (((uintptr_t)x) % al) {
+            set_error(NOTORIOUS_FFT_ERR_INVALID, "device input pointer is not aligned to its element type");
+            goto done;
+        }
+    }
+    if (!yd) {
+        if (!grow(&p->stage_out, &p->stage_out_bytes, out_bytes)) goto done;
+        dout = p->stage_out;
+        if (xd && x == y) {
+            set_error(NOTORIOUS_FFT_ERR_INVALID, "in-place call mixing device and host memory");
+            goto done;
+        }
+    } else {
+        size_t al = out_eb == sizeof(cplx_t) ? sizeof(cplx_t) : sizeof(real_t);
+        if (((uintptr_t)y) % al) {
+            set_error(NOTORIOUS_FFT_ERR_INVALID, "device output pointer is not aligned to its element type");
+            goto done;
+        }
+    }
+    if (plan_execute(p, kind, din, dout, howmany, idist, odist, s, vjp) != 0) goto done;
+    if (!yd) {
+        if (!cuda_ok(cudaMemcpyAsync(y, dout, out_bytes, cudaMemcpyDeviceToHost, s), "D2H copy")) goto done;
+    }
+    if (!xd || !yd) cuda_ok(cudaStreamSynchronize(s), "stream synchronize");
+done:
+    if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- plans ------------------------------------------------------------------
+notorious_fft_aux* notorious_fft_mkaux_dft(int d, int* Ns) { return make_aux(FAM_DFT, d, Ns); }
+notorious_fft_aux* notorious_fft_mkaux_dft_1d(int N) { return make_aux(FAM_DFT, 1, &N); }
+notorious_fft_aux* notorious_fft_mkaux_dft_2d(int N1, int N2) {
+    int Ns[2] = {N1, N2};
+    return make_aux(FAM_DFT, 2, Ns);
+}
+notorious_fft_aux* notorious_fft_mkaux_dft_3d(int N1, int N2, int N3) {
+    int Ns[3] = {N1, N2, N3};
+    return make_aux(FAM_DFT, 3, Ns);
+}
+notorious_fft_aux* notorious_fft_mkaux_realdft(int d, int* Ns) { return make_aux(FAM_REAL, d, Ns); }
+notorious_fft_aux* notorious_fft_mkaux_realdft_1d(int N) { return make_aux(FAM_REAL, 1, &N); }
+notorious_fft_aux* notorious_fft_mkaux_realdft_2d(int N1, int N2) {
+    int Ns[2] = {N1, N2};
+    return make_aux(FAM_REAL, 2, Ns);
+}
+notorious_fft_aux* notorious_fft_mkaux_realdft_3d(int N1, int N2, int N3) {
+    int Ns[3] = {N1, N2, N3};
+    return make_aux(FAM_REAL, 3, Ns);
+}
+notorious_fft_aux* notorious_fft_mkaux_t2t3(int d, int* Ns) { return make_aux(FAM_T2T3, d, Ns); }
+notorious_fft_aux* notorious_fft_mkaux_t2t3_1d(int N) { return make_aux(FAM_T2T3, 1, &N); }
+notorious_fft_aux* notorious_fft_mkaux_t2t3_2d(int N1, int N2) {
+    int Ns[2] = {N1, N2};
+    return make_aux(FAM_T2T3, 2, Ns);
+}
+notorious_fft_aux* notorious_fft_mkaux_t2t3_3d(int N1, int N2, int N3) {
+    int Ns[3] = {N1, N2, N3};
+    return make_aux(FAM_T2T3, 3, Ns);
+}
+notorious_fft_aux* notorious_fft_mkaux_t4(int d, int* Ns) { return make_aux(FAM_T4, d, Ns); }
+notorious_fft_aux* notorious_fft_mkaux_t4_1d(int N) { return make_aux(FAM_T4, 1, &N); }
+notorious_fft_aux* notorious_fft_mkaux_t4_2d(int N1, int N2) {
+    int Ns[2] = {N1, N2};
+    return make_aux(FAM_T4, 2, Ns);
+}
+notorious_fft_aux* notorious_fft_mkaux_t4_3d(int N1, int N2, int N3) {
+    int Ns[3] = {N1, N2, N3};
+    return make_aux(FAM_T4, 3, Ns);
+}
+
+void notorious_fft_free_aux(notorious_fft_aux* a) {
+    if (!a) return;
+    if (a->plan) plan_destroy(a->plan);
+    free(a);
+}
+
+// ---- transforms -------------------------------------------------------------
+void notorious_fft_dft(notorious_fft_cmpl* x, notorious_fft_cmpl* y, const notorious_fft_aux* a) { run(K_DFT, x, y, a, 1, 0, 0, 0); }
+void notorious_fft_invdft(notorious_fft_cmpl* x, notorious_fft_cmpl* y, const notorious_fft_aux* a) { run(K_INVDFT, x, y, a, 1, 0, 0, 0); }
+void notorious_fft_realdft(notorious_fft_real* x, notorious_fft_cmpl* z, const notorious_fft_aux* a) { run(K_REALDFT, x, z, a, 1, 0, 0, 0); }
+void notorious_fft_invrealdft(notorious_fft_cmpl* z, notorious_fft_real* y, const notorious_fft_aux* a) { run(K_INVREALDFT, z, y, a, 1, 0, 0, 0); }
+void notorious_fft_dct2(notorious_fft_real* x, notorious_fft_real* y, const notorious_fft_aux* a) { run(K_DCT2, x, y, a, 1, 0, 0, 0); }
+void notorious_fft_dst2(notorious_fft_real* x, notorious_fft_real* y, const notorious_fft_aux* a) { run(K_DST2, x, y, a, 1, 0, 0, 0); }
+void notorious_fft_dct3(notorious_fft_real* x, notorious_fft_real* y, const notorious_fft_aux* a) { run(K_DCT3, x, y, a, 1, 0, 0, 0); }
+void notorious_fft_dst3(notorious_fft_real* x, notorious_fft_real* y, const notorious_fft_aux* a) { run(K_DST3, x, y, a, 1, 0, 0, 0); }
+void notorious_fft_dct4(notorious_fft_real* x, notorious_fft_real* y, const notorious_fft_aux* a) { run(K_DCT4, x, y, a, 1, 0, 0, 0); }
+void notorious_fft_dst4(notorious_fft_real* x, notorious_fft_real* y, const notorious_fft_aux* a) { run(K_DST4, x, y, a, 1, 0, 0, 0); }
+
+void notorious_fft_execute_batched(int kind, void* x, void* y, const notorious_fft_aux* a, int howmany, ptrdiff_t idist,
+                                   ptrdiff_t odist) {
+    if (kind < 0 || kind > 9) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "unknown transform kind %d", kind);
+        return;
+    }
+    run(kind, x, y, a, howmany, idist, odist, 0);
+}
+
+#define NFFT_BATCHED(name, K, TI, TO)                                                                               \
+    void notorious_fft_##name##_batched(TI* x, TO* y, const notorious_fft_aux* a, int howmany, ptrdiff_t idist,    \
+                                        ptrdiff_t odist) {                                                          \
+        run(K, x, y, a, howmany, idist, odist, 0);                                                                  \
+    }
+NFFT_BATCHED(dft, K_DFT, notorious_fft_cmpl, notorious_fft_cmpl)
+NFFT_BATCHED(invdft, K_INVDFT, notorious_fft_cmpl, notorious_fft_cmpl)
+NFFT_BATCHED(realdft, K_REALDFT, notorious_fft_real, notorious_fft_cmpl)
+NFFT_BATCHED(invrealdft, K_INVREALDFT, notorious_fft_cmpl, notorious_fft_real)
+NFFT_BATCHED(dct2, K_DCT2, notorious_fft_real, notorious_fft_real)
+NFFT_BATCHED(dst2, K_DST2, notorious_fft_real, notorious_fft_real)
+NFFT_BATCHED(dct3, K_DCT3, notorious_fft_real, notorious_fft_real)
+NFFT_BATCHED(dst3, K_DST3, notorious_fft_real, notorious_fft_real)
+NFFT_BATCHED(dct4, K_DCT4, notorious_fft_real, notorious_fft_real)
+NFFT_BATCHED(dst4, K_DST4, notorious_fft_real, notorious_fft_real)
+#undef NFFT_BATCHED
+
+// ---- adjoints ---------------------------------------------------------------
+void notorious_fft_dft_vjp(notorious_fft_cmpl* g, notorious_fft_cmpl* gx, const notorious_fft_aux* a) { run(K_DFT, g, gx, a, 1, 0, 0, 1); }
+void notorious_fft_invdft_vjp(notorious_fft_cmpl* g, notorious_fft_cmpl* gx, const notorious_fft_aux* a) { run(K_INVDFT, g, gx, a, 1, 0, 0, 1); }
+void notorious_fft_realdft_vjp(notorious_fft_cmpl* g, notorious_fft_real* gx, const notorious_fft_aux* a) { run(K_REALDFT, g, gx, a, 1, 0, 0, 1); }
+void notorious_fft_invrealdft_vjp(notorious_fft_real* g, notorious_fft_cmpl* gz, const notorious_fft_aux* a) { run(K_INVREALDFT, g, gz, a, 1, 0, 0, 1); }
+void notorious_fft_dct2_vjp(notorious_fft_real* g, notorious_fft_real* gx, const notorious_fft_aux* a) { run(K_DCT2, g, gx, a, 1, 0, 0, 1); }
+void notorious_fft_dst2_vjp(notorious_fft_real* g, notorious_fft_real* gx, const notorious_fft_aux* a) { run(K_DST2, g, gx, a, 1, 0, 0, 1); }
+void notorious_fft_dct3_vjp(notorious_fft_real* g, notorious_fft_real* gx, const notorious_fft_aux* a) { run(K_DCT3, g, gx, a, 1, 0, 0, 1); }
+void notorious_fft_dst3_vjp(notorious_fft_real* g, notorious_fft_real* gx, const notorious_fft_aux* a) { run(K_DST3, g, gx, a, 1, 0, 0, 1); }
+void notorious_fft_dct4_vjp(notorious_fft_real* g, notorious_fft_real* gx, const notorious_fft_aux* a) { run(K_DCT4, g, gx, a, 1, 0, 0, 1); }
+void notorious_fft_dst4_vjp(notorious_fft_real* g, notorious_fft_real* gx, const notorious_fft_aux* a) { run(K_DST4, g, gx, a, 1, 0, 0, 1); }
+
+void notorious_fft_vjp_batched(int kind, void* g, void* gx, const notorious_fft_aux* a, int howmany, ptrdiff_t idist,
+                               ptrdiff_t odist) {
+    if (kind < 0 || kind > 9) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "unknown transform kind %d", kind);
+        return;
+    }
+    run(kind, g, gx, a, howmany, idist, odist, 1);
+}
+
+// ---- errors / streams / info -------------------------------------------------
+int notorious_fft_last_error(void) { return last_error(); }
+const char* notorious_fft_last_error_string(void) { return last_error_string(); }
+void notorious_fft_clear_error(void) { clear_error(); }
+
+void notorious_fft_set_stream(void* stream) { t_stream = (cudaStream_t)stream; }
+void* notorious_fft_get_stream(void) { return (void*)t_stream; }
+int notorious_fft_synchronize(void) {
+    clear_error();
+    if (!cuda_ok(cudaStreamSynchronize(t_stream), "cudaStreamSynchronize")) return last_error();
+    return 0;
+}
+
+int notorious_fft_set_form(notorious_fft_aux* a, int form) {
+    clear_error();
+    if (!a || !a->plan) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "NULL aux");
+        return NOTORIOUS_FFT_ERR_INVALID;
+    }
+    if (form == NOTORIOUS_FFT_FORM_PLAIN) {
+        a->plan->form = form;
+        return 0;
+    }
+    if (form == NOTORIOUS_FFT_FORM_SPLIT_TC) {
+        set_error(NOTORIOUS_FFT_ERR_UNSUPPORTED, "the split tensor-core form is not available in this build");
+        return NOTORIOUS_FFT_ERR_UNSUPPORTED;
+    }
+    set_error(NOTORIOUS_FFT_ERR_INVALID, "unknown form %d", form);
+    return NOTORIOUS_FFT_ERR_INVALID;
+}
+int notorious_fft_get_form(const notorious_fft_aux* a) { return (a && a->plan) ? a->plan->form : -1; }
+
+int notorious_fft_real_size(void) { return (int)sizeof(real_t); }
+long long notorious_fft_launch_count(void) { return launch_count(); }
+const char* notorious_fft_version(void) { return "notorious-fft-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

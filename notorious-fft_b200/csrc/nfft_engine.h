@@ -1,0 +1,148 @@
+// nfft_engine.h -- host-side engine of the B200 FFT library (internal).
+//
+// A plan (struct notorious_fft_plan) is a list of axis steps.  Each step runs
+// one 1-D transform along one axis of a strided view, as one or more Stockham
+// passes (nfft_pass.cuh), with the transform family's pre/post operators fused
+// into the first and last pass.  Power-of-two axes use the passes directly;
+// other complex axes use Bluestein (chirp premultiply fused into the first
+// forward pass, filter product + first inverse pass fused into the last
+// forward pass, window + chirp postmultiply fused into the last inverse pass).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "nfft_pass.cuh"
+
+#ifndef NFFT_REAL
+#define NFFT_REAL double
+#endif
+
+namespace nfft {
+
+using real_t = NFFT_REAL;
+using cplx_t = C2<real_t>;
+
+// ---- errors ---------------------------------------------------------------
+void set_error(int code, const char* fmt, ...);
+int last_error();
+const char* last_error_string();
+void clear_error();
+bool cuda_ok(cudaError_t e, const char* what);
+
+// ---- per-device context ---------------------------------------------------
+struct DeviceCtx {
+    int device = -1;
+    int sm_count = 0;
+    size_t l2_bytes = 0;
+    TwTables<real_t>* tw = nullptr;   // device twiddle tables
+    bool ready = false;
+};
+DeviceCtx* device_ctx(int device);   // initializes on first use (tables, kernel attributes)
+DeviceCtx* current_ctx();            // context of the calling thread's current device, or null
+
+// ---- transform families / kinds ---------------------------------------------
+enum Family { FAM_DFT = 0, FAM_REAL = 1, FAM_T2T3 = 2, FAM_T4 = 3 };
+enum Kind {
+    K_DFT = 0, K_INVDFT = 1, K_REALDFT = 2, K_INVREALDFT = 3,
+    K_DCT2 = 4, K_DST2 = 5, K_DCT3 = 6, K_DST3 = 7, K_DCT4 = 8, K_DST4 = 9
+};
+Family family_of(int kind);
+
+// ---- strided views ----------------------------------------------------------
+// Lines of one axis: element e of line (b0, b1, ...) lives at
+//   ptr + sum_d b_d * str[d] + e * estride        (units: elements of the view type)
+constexpr int MAX_BATCH_DIMS = 3;
+struct View {
+    void* ptr = nullptr;
+    long long estride = 1;
+    int nb = 0;                          // batch dims, innermost first
+    long long cnt[MAX_BATCH_DIMS] = {1, 1, 1};
+    long long str[MAX_BATCH_DIMS] = {0, 0, 0};
+    long long lines() const {
+        long long n = 1;
+        for (int i = 0; i < nb; ++i) n *= cnt[i];
+        return n;
+    }
+};
+
+// ---- power-of-two complex FFT schedule ------------------------------------
+struct FftSchedule {
+    int logL = 0;
+    int npass = 0;
+    int plog[4] = {0, 0, 0, 0};      // pass radices (log2), in execution order
+    int tile[4] = {12, 12, 12, 12};  // log2 tile size of each pass
+    int nsub[4] = {0, 0, 0, 0};
+    int sub[4][MAX_SUB] = {};
+};
+// strided: the axis is not contiguous (every pass runs in column mode).
+FftSchedule make_schedule(int logL, bool strided);
+FftSchedule reversed(const FftSchedule& s);
+
+// ---- one axis of a plan -------------------------------------------------------
+struct AxisPlan {
+    int n = 1;                 // axis length (real length for the real families)
+    bool pow2 = true;
+    int logn = 0;
+    // power-of-two inner complex FFT (length n for dft, n/2 for the real families)
+    FftSchedule fft_contig, fft_strided;
+    // Bluestein (complex family, n not a power of two)
+    int logM = 0;
+    cplx_t* chirp = nullptr;   // e^{-i pi k^2/n}, k < n
+    cplx_t* filt = nullptr;    // FFT_M(conj chirp, wrapped) / M
+    FftSchedule mfwd, minv;    // M-point forward schedule and its reverse
+};
+
+}  // namespace nfft
+
+// The plan behind notorious_fft_aux::plan.
+struct notorious_fft_plan {
+    int family = 0;
+    int device = -1;
+    std::vector<int> dims;            // Ns[0] slowest
+    std::vector<nfft::AxisPlan> axes;
+    int form = 0;                     // precision form (NOTORIOUS_FFT_FORM_*)
+    // scratch (device), grown on demand; [0],[1] ping-pong of multi-pass axes
+    void* scratch[2] = {nullptr, nullptr};
+    size_t scratch_bytes[2] = {0, 0};
+    // device staging for host-pointer calls
+    void* stage_in = nullptr;
+    void* stage_out = nullptr;
+    size_t stage_in_bytes = 0, stage_out_bytes = 0;
+    // temporary of the multi-dimensional inverse real transform
+    void* nd_tmp = nullptr;
+    size_t nd_tmp_bytes = 0;
+    std::mutex mu;
+};
+
+namespace nfft {
+
+notorious_fft_plan* plan_create(int family, int d, const int* Ns);
+void plan_destroy(notorious_fft_plan* p);
+// Elements (of the family's input / output type) of one transform.
+long long plan_in_elems(const notorious_fft_plan* p, int kind);
+long long plan_out_elems(const notorious_fft_plan* p, int kind);
+// Element sizes (bytes) of the input / output type of `kind`.
+size_t in_elem_bytes(int kind);
+size_t out_elem_bytes(int kind);
+// Run `kind` on device pointers (asynchronous on `stream`).  Returns 0 on success.
+// vjp != 0 runs the adjoint of `kind` (input: the cotangent of its output).
+int plan_execute(notorious_fft_plan* p, int kind, const void* in, void* out, long long howmany,
+                 long long idist, long long odist, cudaStream_t stream, int vjp = 0);
+
+// Kernel launchers (nfft_kernels.cu)
+bool launch_pass(const PassArgs& a, int load_op, int store_op, int log_tile, long long ntiles, cudaStream_t s);
+bool launch_unpack(const PassArgs& a, int store_op, const cplx_t* Z, long long zdist, long long nlines, cudaStream_t s);
+bool launch_tiny(const real_t* x, real_t* y, long long howmany, long long inner, long long idist, long long odist,
+                 int in_cplx, int out_cplx, double factor, cudaStream_t s);
+bool launch_init_tables(TwTables<real_t>* tw, cudaStream_t s);
+bool launch_chirp(cplx_t* chirp, cplx_t* bwrap, long long n, long long M, cudaStream_t s);
+bool set_kernel_attributes();
+long long launch_count();
+
+}  // namespace nfft

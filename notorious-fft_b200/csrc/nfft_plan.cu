@@ -1,0 +1,822 @@
+// nfft_plan.cu -- device contexts, error state, pass schedules, plan
+// construction and execution.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "nfft_engine.h"
+
+namespace nfft {
+
+// ---------------------------------------------------------------------------
+// errors (per calling thread)
+// ---------------------------------------------------------------------------
+static thread_local int t_err = 0;
+static thread_local char t_errmsg[512] = "";
+
+void set_error(int code, const char* fmt, ...) {
+    t_err = code;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_errmsg, sizeof t_errmsg, fmt, ap);
+    va_end(ap);
+}
+int last_error() { return t_err; }
+const char* last_error_string() { return t_errmsg; }
+void clear_error() {
+    t_err = 0;
+    t_errmsg[0] = 0;
+}
+bool cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(e == cudaErrorMemoryAllocation ? 3 : 4, "%s: %s", what, cudaGetErrorString(e));
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// per-device contexts
+// ---------------------------------------------------------------------------
+static std::mutex g_ctx_mu;
+static DeviceCtx g_ctx[64];
+
+DeviceCtx* device_ctx(int device) {
+    if (device < 0 || device >= 64) {
+        set_error(2, "device %d out of range", device);
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    DeviceCtx& c = g_ctx[device];
+    if (c.ready) return &c;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return nullptr;
+    cudaDeviceProp prop;
+    if (!cuda_ok(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties")) return nullptr;
+    if (prop.major < 10) {
+        set_error(2, "device %d (%s, sm_%d%d) is not an sm_100 GPU", device, prop.name, prop.major, prop.minor);
+        return nullptr;
+    }
+    c.device = device;
+    c.sm_count = prop.multiProcessorCount;
+    c.l2_bytes = (size_t)prop.l2CacheSize;
+    if (!cuda_ok(cudaMalloc((void**)&c.tw, sizeof(TwTables<real_t>)), "cudaMalloc(twiddle tables)")) return nullptr;
+    if (!launch_init_tables(c.tw, 0)) return nullptr;
+    if (!set_kernel_attributes()) return nullptr;
+    if (!cuda_ok(cudaDeviceSynchronize(), "twiddle table init")) return nullptr;
+    c.ready = true;
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    return &c;
+}
+
+DeviceCtx* current_ctx() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        set_error(2, "no CUDA device available");
+        return nullptr;
+    }
+    return device_ctx(dev);
+}
+
+Family family_of(int kind) {
+    switch (kind) {
+    case K_DFT: case K_INVDFT: return FAM_DFT;
+    case K_REALDFT: case K_INVREALDFT: return FAM_REAL;
+    case K_DCT4: case K_DST4: return FAM_T4;
+    default: return FAM_T2T3;
+    }
+}
+
+size_t in_elem_bytes(int kind) {
+    return (kind == K_DFT || kind == K_INVDFT || kind == K_INVREALDFT) ? sizeof(cplx_t) : sizeof(real_t);
+}
+size_t out_elem_bytes(int kind) {
+    return (kind == K_DFT || kind == K_INVDFT || kind == K_REALDFT) ? sizeof(cplx_t) : sizeof(real_t);
+}
+
+// ---------------------------------------------------------------------------
+// schedules
+// ---------------------------------------------------------------------------
+static int ilog2(long long n) {
+    int l = 0;
+    while ((1ll << l) < n) ++l;
+    return l;
+}
+static bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// Minimum lines per tile in column mode: 64 contiguous bytes per row.
+static int log_jmin() { return sizeof(real_t) == 8 ? 2 : 3; }
+
+static void split_sub(int logR, int* nsub, int* sub) {
+    int n = 0;
+    if (logR == 0) {
+        *nsub = 0;
+        return;
+    }
+    int n4 = logR / 4, rem = logR % 4;
+    if (rem == 1 && n4 >= 1) {
+        for (int i = 0; i < n4 - 1; ++i) sub[n++] = 4;
+        sub[n++] = 3;
+        sub[n++] = 2;
+    } else {
+        for (int i = 0; i < n4; ++i) sub[n++] = 4;
+        if (rem) sub[n++] = rem;
+    }
+    *nsub = n;
+}
+
+FftSchedule make_schedule(int logL, bool strided) {
+    FftSchedule s;
+    s.logL = logL;
+    const int max_tile = 13;
+    const int jmin = log_jmin();
+    if (!strided && logL <= max_tile) {
+        s.npass = 1;
+        s.plog[0] = logL;
+        s.tile[0] = logL <= 12 ? 12 : 13;
+    } else {
+        const int maxr = max_tile - jmin;
+        int np = (logL + maxr - 1) / maxr;
+        if (np < 1) np = 1;
+        s.npass = np;
+        int base = logL / np, extra = logL % np;
+        for (int i = 0; i < np; ++i) s.plog[i] = base + (i < extra ? 1 : 0);
+        for (int i = 0; i < np; ++i) s.tile[i] = (s.plog[i] + jmin + 1 <= 12) ? 12 : 13;
+    }
+    for (int i = 0; i < s.npass; ++i) split_sub(s.plog[i], &s.nsub[i], s.sub[i]);
+    return s;
+}
+
+FftSchedule reversed(const FftSchedule& s) {
+    FftSchedule r = s;
+    for (int i = 0; i < s.npass; ++i) {
+        int k = s.npass - 1 - i;
+        r.plog[i] = s.plog[k];
+        r.tile[i] = s.tile[k];
+        r.nsub[i] = s.nsub[k];
+        for (int j = 0; j < MAX_SUB; ++j) r.sub[i][j] = s.sub[k][j];
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// scratch
+// ---------------------------------------------------------------------------
+static void* get_scratch(notorious_fft_plan* p, int slot, size_t bytes) {
+    if (p->scratch_bytes[slot] >= bytes && p->scratch[slot]) return p->scratch[slot];
+    if (p->scratch[slot]) {
+        cudaFree(p->scratch[slot]);
+        p->scratch[slot] = nullptr;
+        p->scratch_bytes[slot] = 0;
+    }
+    void* ptr = nullptr;
+    if (!cuda_ok(cudaMalloc(&ptr, bytes), "cudaMalloc(scratch)")) return nullptr;
+    p->scratch[slot] = ptr;
+    p->scratch_bytes[slot] = bytes;
+    return ptr;
+}
+
+static size_t scratch_cap_bytes() {
+    static size_t cap = 0;
+    if (!cap) {
+        const char* e = getenv("NOTORIOUS_FFT_SCRATCH_MB");
+        long mb = e ? atol(e) : 64;
+        if (mb < 1) mb = 1;
+        cap = (size_t)mb << 20;
+    }
+    return cap;
+}
+
+// ---------------------------------------------------------------------------
+// pass construction
+// ---------------------------------------------------------------------------
+struct OpSpec {
+    int ld = LD_C, st = ST_C;
+    int conj_in = 0, conj_out = 0;
+    double scale = 1.0;
+    long long N = 0;
+    int logN = 0;
+    int dst = 0;
+    bool paired = false;   // st is ST_R / ST_T2 (needs whole lines or the unpack epilogue)
+    int vjp = 0;           // adjoint weights of the real operators
+};
+
+static void fill_common(PassArgs& a, const DeviceCtx* c) {
+    memset(&a, 0, sizeof a);
+    a.tw = c->tw;
+    a.scale = 1.0;
+    a.jpos = -1;
+}
+
+// Line dims of a pass.  Contiguous lines: j innermost then the batch dims;
+// strided lines: the view's first (unit-stride) batch dim innermost, then j.
+static void set_lines(PassArgs& a, const View& src, const View& dst, long long nj, bool j_inner) {
+    int nd = 0;
+    auto add_batch = [&](int d) {
+        a.cnt[nd] = src.cnt[d];
+        a.istr[nd] = src.str[d];
+        a.ostr[nd] = dst.str[d];
+        ++nd;
+    };
+    auto add_j = [&]() {
+        if (nj > 1) {
+            a.cnt[nd] = nj;
+            a.istr[nd] = 0;
+            a.ostr[nd] = 0;
+            a.jpos = nd;
+            ++nd;
+        }
+    };
+    if (j_inner) {
+        add_j();
+        for (int d = 0; d < src.nb; ++d) add_batch(d);
+    } else {
+        if (src.nb > 0) add_batch(0);
+        add_j();
+        for (int d = 1; d < src.nb; ++d) add_batch(d);
+    }
+    if (nd == 0) {
+        a.cnt[0] = 1;
+        a.istr[0] = a.ostr[0] = 0;
+        nd = 1;
+    }
+    a.ndims = nd;
+    long long n = 1;
+    for (int i = 0; i < nd; ++i) n *= a.cnt[i];
+    a.nlines = n;
+}
+
+static bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR, int tile,
+                     int nsub, const int* sub, const OpSpec& op, bool first, bool last, int mid, int logNs_out,
+                     const cplx_t* chirp, const cplx_t* filt, cudaStream_t s) {
+    PassArgs a;
+    fill_common(a, c);
+    a.in = src.ptr;
+    a.out = dst.ptr;
+    a.logR = logR;
+    a.logNs = logNs;
+    a.logNj = logL - logR;
+    a.logNs_out = logNs_out;
+    a.nsub = nsub;
+    for (int i = 0; i < nsub; ++i) a.sublog[i] = sub[i];
+    a.in_estride = src.estride;
+    a.out_estride = dst.estride;
+    const long long nj = 1ll << (logL - logR);
+    // Strided source axis with a unit-stride batch dim: that dim goes innermost
+    // so consecutive lines are consecutive addresses; otherwise j goes innermost.
+    const bool j_inner = !(src.estride != 1 && src.nb > 0 && src.str[0] == 1);
+    set_lines(a, src, dst, nj, j_inner);
+    a.in_row = (nj == 1 && src.estride == 1) ? 1 : 0;
+    a.out_row = (logNs_out == 0 && dst.estride == 1 && (nj == 1 || j_inner)) ? 1 : 0;
+    a.conj_in = first ? op.conj_in : 0;
+    a.conj_out = last ? op.conj_out : 0;
+    a.scale = last ? op.scale : 1.0;
+    a.N = op.N;
+    a.logN = op.logN;
+    a.dst = op.dst;
+    a.chirp = chirp;
+    a.filt = filt;
+    a.mid = mid;
+    a.vjp = op.vjp;
+    int ldop = first ? op.ld : LD_C;
+    int stop = last ? op.st : ST_C;
+    int logE_max = tile;
+    int logJ = logE_max - logR;
+    if (logJ > 8) logJ = 8;
+    int lines_log = ilog2(a.nlines);
+    if (logJ > lines_log) logJ = lines_log;
+    if (logJ < 0) {
+        set_error(6, "pass radix 2^%d exceeds tile 2^%d", logR, tile);
+        return false;
+    }
+    a.logJ = logJ;
+    long long ntiles = (a.nlines + (1ll << logJ) - 1) >> logJ;
+    return launch_pass(a, ldop, stop, tile, ntiles, s);
+}
+
+// Scratch view with the same lines as `like` and a contiguous (or, for
+// strided lines, unit-stride-batch-innermost) layout of axis length L.
+static View scratch_view(void* ptr, const View& like, long long L, bool strided) {
+    View v;
+    v.ptr = ptr;
+    v.nb = like.nb;
+    for (int d = 0; d < like.nb; ++d) v.cnt[d] = like.cnt[d];
+    if (!strided || like.nb == 0) {
+        v.estride = 1;
+        long long s = L;
+        for (int d = 0; d < like.nb; ++d) {
+            v.str[d] = s;
+            s *= like.cnt[d];
+        }
+    } else {
+        v.str[0] = 1;
+        v.estride = like.cnt[0];
+        long long s = like.cnt[0] * L;
+        for (int d = 1; d < like.nb; ++d) {
+            v.str[d] = s;
+            s *= like.cnt[d];
+        }
+    }
+    return v;
+}
+
+// Run a power-of-two FFT of complex length 2^logL over the lines of src ->
+// dst with the fused operators of `op`.  Multi-pass runs go through plan
+// scratch slots 0/1, in chunks of the outermost batch dim sized to the
+// scratch cap.
+static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisPlan& ax, View src, View dst,
+                          const OpSpec& op, cudaStream_t s) {
+    const int logL = ax.fft_contig.logL;
+    const bool strided = !(src.estride == 1 && dst.estride == 1);
+    const FftSchedule& sch = strided ? ax.fft_strided : ax.fft_contig;
+    const long long L = 1ll << logL;
+    const int np = sch.npass;
+    if (np == 1 && !(op.paired && strided)) {
+        return run_pass(c, src, dst, logL, 0, sch.plog[0], sch.tile[0], sch.nsub[0], sch.sub[0], op, true, true, 0, 0,
+                        nullptr, nullptr, s);
+    }
+    // multi-pass (or a paired op on strided lines): chunk the outermost batch dim
+    long long lines = src.lines();
+    long long outer = src.nb > 0 ? src.cnt[src.nb - 1] : 1;
+    long long inner_lines = outer > 0 ? lines / outer : lines;
+    size_t per_outer = (size_t)inner_lines * (size_t)L * sizeof(cplx_t);
+    long long chunk = (long long)(scratch_cap_bytes() / std::max<size_t>(per_outer, 1));
+    if (chunk < 1) chunk = 1;
+    if (chunk > outer) chunk = outer;
+    const bool paired_epilogue = op.paired;
+    const int nbuf = paired_epilogue ? (np >= 2 ? 2 : 1) : (np >= 3 ? 2 : 1);
+    void* buf[2] = {nullptr, nullptr};
+    for (int i = 0; i < nbuf; ++i) {
+        buf[i] = get_scratch(p, i, (size_t)chunk * per_outer);
+        if (!buf[i]) return false;
+    }
+    for (long long o0 = 0; o0 < outer; o0 += chunk) {
+        long long cn = std::min(chunk, outer - o0);
+        View vs = src, vd = dst;
+        if (src.nb > 0) {
+            vs.ptr = (char*)src.ptr + (size_t)(o0 * src.str[src.nb - 1]) * (op.ld == LD_C || op.ld == LD_BLUE || op.ld == LD_IR ? sizeof(cplx_t) : sizeof(real_t));
+            vs.cnt[src.nb - 1] = cn;
+            vd.ptr = (char*)dst.ptr + (size_t)(o0 * dst.str[dst.nb - 1]) *
+                                          ((op.st == ST_C || op.st == ST_R || op.st == ST_BLUE) ? sizeof(cplx_t) : sizeof(real_t));
+            vd.cnt[dst.nb - 1] = cn;
+        }
+        View cur = vs;
+        int logNs = 0;
+        for (int i = 0; i < np; ++i) {
+            bool first = i == 0, last = i == np - 1;
+            View out;
+            bool to_user = last && !paired_epilogue;
+            if (to_user) out = vd;
+            else out = scratch_view(buf[i % nbuf], vs, L, strided && !paired_epilogue);
+            OpSpec o = op;
+            if (last && paired_epilogue) {
+                o.st = ST_C;
+                o.scale = 1.0;
+                o.conj_out = 0;
+            }
+            int logR = sch.plog[i];
+            if (!run_pass(c, cur, out, logL, logNs, logR, sch.tile[i], sch.nsub[i], sch.sub[i], o, first, last, 0, logNs,
+                          nullptr, nullptr, s))
+                return false;
+            logNs += logR;
+            cur = out;
+        }
+        if (paired_epilogue) {
+            PassArgs a;
+            fill_common(a, c);
+            a.out = vd.ptr;
+            a.out_estride = vd.estride;
+            a.N = op.N;
+            a.logN = op.logN;
+            a.dst = op.dst;
+            a.vjp = op.vjp;
+            a.ndims = vd.nb > 0 ? vd.nb : 1;
+            for (int d = 0; d < vd.nb; ++d) {
+                a.cnt[d] = vd.cnt[d];
+                a.ostr[d] = vd.str[d];
+            }
+            if (vd.nb == 0) {
+                a.cnt[0] = 1;
+                a.ostr[0] = 0;
+            }
+            if (!launch_unpack(a, op.st, (const cplx_t*)cur.ptr, L, vs.lines(), s)) return false;
+        }
+    }
+    return true;
+}
+
+// Bluestein for a complex axis of length n (not a power of two).
+static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisPlan& ax, View src, View dst,
+                               int inverse, double scale, cudaStream_t s) {
+    const int logM = ax.logM;
+    const long long M = 1ll << logM;
+    OpSpec op;
+    op.ld = LD_BLUE;
+    op.st = ST_BLUE;
+    op.conj_in = inverse;
+    op.conj_out = inverse;
+    op.scale = scale;
+    op.N = ax.n;
+    const FftSchedule& f = ax.mfwd;
+    const FftSchedule& g = ax.minv;
+    const int np = f.npass;
+    if (np == 1) {
+        return run_pass(c, src, dst, logM, 0, f.plog[0], f.tile[0], f.nsub[0], f.sub[0], op, true, true, 1, 0, ax.chirp,
+                        ax.filt, s);
+    }
+    long long lines = src.lines();
+    long long outer = src.nb > 0 ? src.cnt[src.nb - 1] : 1;
+    long long inner_lines = outer > 0 ? lines / outer : lines;
+    size_t per_outer = (size_t)inner_lines * (size_t)M * sizeof(cplx_t);
+    long long chunk = (long long)(scratch_cap_bytes() / std::max<size_t>(per_outer, 1));
+    if (chunk < 1) chunk = 1;
+    if (chunk > outer) chunk = outer;
+    void* buf[2];
+    for (int i = 0; i < 2; ++i) {
+        buf[i] = get_scratch(p, i, (size_t)chunk * per_outer);
+        if (!buf[i]) return false;
+    }
+    for (long long o0 = 0; o0 < outer; o0 += chunk) {
+        long long cn = std::min(chunk, outer - o0);
+        View vs = src, vd = dst;
+        if (src.nb > 0) {
+            vs.ptr = (cplx_t*)src.ptr + o0 * src.str[src.nb - 1];
+            vs.cnt[src.nb - 1] = cn;
+            vd.ptr = (cplx_t*)dst.ptr + o0 * dst.str[dst.nb - 1];
+            vd.cnt[dst.nb - 1] = cn;
+        }
+        View cur = vs;
+        int bi = 0;
+        int logNs = 0;
+        // forward passes 0 .. np-2
+        for (int i = 0; i < np - 1; ++i) {
+            View out = scratch_view(buf[bi], vs, M, false);
+            if (!run_pass(c, cur, out, logM, logNs, f.plog[i], f.tile[i], f.nsub[i], f.sub[i], op, i == 0, false, 0,
+                          logNs, ax.chirp, ax.filt, s))
+                return false;
+            logNs += f.plog[i];
+            cur = out;
+            bi ^= 1;
+        }
+        // last forward pass + filter + first inverse pass
+        {
+            View out = scratch_view(buf[bi], vs, M, false);
+            OpSpec o = op;
+            if (!run_pass(c, cur, out, logM, logNs, f.plog[np - 1], f.tile[np - 1], f.nsub[np - 1], f.sub[np - 1], o,
+                          false, false, 1, 0, ax.chirp, ax.filt, s))
+                return false;
+            cur = out;
+            bi ^= 1;
+        }
+        // remaining inverse passes (the first one was fused above)
+        int logNs_inv = g.plog[0];
+        for (int i = 1; i < np; ++i) {
+            bool last = i == np - 1;
+            View out = last ? vd : scratch_view(buf[bi], vs, M, false);
+            if (!run_pass(c, cur, out, logM, logNs_inv, g.plog[i], g.tile[i], g.nsub[i], g.sub[i], op, false, last, 0,
+                          logNs_inv, ax.chirp, ax.filt, s))
+                return false;
+            logNs_inv += g.plog[i];
+            cur = out;
+            bi ^= 1;
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// plans
+// ---------------------------------------------------------------------------
+static bool build_axis(notorious_fft_plan* p, const DeviceCtx* c, AxisPlan& ax, int n, int family) {
+    ax.n = n;
+    ax.pow2 = is_pow2(n);
+    ax.logn = ilog2(n);
+    if (ax.pow2) {
+        int logL = (family == FAM_DFT) ? ax.logn : std::max(0, ax.logn - 1);
+        ax.fft_contig = make_schedule(logL, false);
+        ax.fft_strided = make_schedule(logL, true);
+        return true;
+    }
+    if (family != FAM_DFT) {
+        set_error(1, "length %d is not a power of two", n);
+        return false;
+    }
+    long long M = 1;
+    while (M < 2ll * n - 1) M <<= 1;
+    ax.logM = ilog2(M);
+    ax.mfwd = make_schedule(ax.logM, false);
+    ax.minv = reversed(ax.mfwd);
+    if (!cuda_ok(cudaMalloc((void**)&ax.chirp, sizeof(cplx_t) * (size_t)n), "cudaMalloc(chirp)")) return false;
+    if (!cuda_ok(cudaMalloc((void**)&ax.filt, sizeof(cplx_t) * (size_t)M), "cudaMalloc(filter)")) return false;
+    cplx_t* bwrap = nullptr;
+    if (!cuda_ok(cudaMalloc((void**)&bwrap, sizeof(cplx_t) * (size_t)M), "cudaMalloc(bluestein kernel)")) return false;
+    bool ok = launch_chirp(ax.chirp, bwrap, n, M, 0);
+    if (ok) {
+        // filt = FFT_M(bwrap) / M with the library's own passes
+        AxisPlan mp;
+        mp.n = (int)M;
+        mp.logn = ax.logM;
+        mp.fft_contig = make_schedule(ax.logM, false);
+        mp.fft_strided = mp.fft_contig;
+        View vs, vd;
+        vs.ptr = bwrap;
+        vd.ptr = ax.filt;
+        OpSpec op;
+        op.scale = 1.0 / (double)M;
+        ok = run_pow2_axis(p, c, mp, vs, vd, op, 0);
+    }
+    ok = ok && cuda_ok(cudaDeviceSynchronize(), "Bluestein filter");
+    cudaFree(bwrap);
+    return ok;
+}
+
+notorious_fft_plan* plan_create(int family, int d, const int* Ns) {
+    if (d < 1 || !Ns) {
+        set_error(1, "invalid rank %d", d);
+        return nullptr;
+    }
+    long long total = 1;
+    for (int i = 0; i < d; ++i) {
+        if (Ns[i] <= 0) {
+            set_error(1, "invalid dimension %d", Ns[i]);
+            return nullptr;
+        }
+        if (family != FAM_DFT && !is_pow2(Ns[i])) {
+            set_error(1, "dimension %d is not a power of two", Ns[i]);
+            return nullptr;
+        }
+        total *= Ns[i];
+        if (total > 0x7fffffffll) {
+            set_error(1, "transform size exceeds the int range of the API");
+            return nullptr;
+        }
+    }
+    DeviceCtx* c = current_ctx();
+    if (!c) return nullptr;
+    notorious_fft_plan* p = new notorious_fft_plan();
+    p->family = family;
+    p->device = c->device;
+    p->dims.assign(Ns, Ns + d);
+    p->axes.resize(d);
+    for (int i = 0; i < d; ++i) {
+        // a real plan transforms only its last axis as real; the leading axes
+        // are full-length complex DFTs of the half spectrum (FFTW layout)
+        int fam_i = (family == FAM_REAL && i < d - 1) ? FAM_DFT : family;
+        if (!build_axis(p, c, p->axes[i], Ns[i], fam_i)) {
+            plan_destroy(p);
+            return nullptr;
+        }
+    }
+    return p;
+}
+
+void plan_destroy(notorious_fft_plan* p) {
+    if (!p) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (p->device >= 0 && prev != p->device) cudaSetDevice(p->device);
+    for (auto& ax : p->axes) {
+        if (ax.chirp) cudaFree(ax.chirp);
+        if (ax.filt) cudaFree(ax.filt);
+    }
+    for (int i = 0; i < 2; ++i)
+        if (p->scratch[i]) cudaFree(p->scratch[i]);
+    if (p->stage_in) cudaFree(p->stage_in);
+    if (p->nd_tmp) cudaFree(p->nd_tmp);
+    if (p->stage_out) cudaFree(p->stage_out);
+    if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
+    delete p;
+}
+
+static long long prod(const std::vector<int>& v, int a, int b) {
+    long long r = 1;
+    for (int i = a; i < b; ++i) r *= v[i];
+    return r;
+}
+
+long long plan_in_elems(const notorious_fft_plan* p, int kind) {
+    long long total = prod(p->dims, 0, (int)p->dims.size());
+    if (kind == K_INVREALDFT) return total / p->dims.back() * (p->dims.back() / 2 + 1);
+    return total;
+}
+long long plan_out_elems(const notorious_fft_plan* p, int kind) {
+    long long total = prod(p->dims, 0, (int)p->dims.size());
+    if (kind == K_REALDFT) return total / p->dims.back() * (p->dims.back() / 2 + 1);
+    return total;
+}
+
+// View of axis `a` of a row-major array with dims D (elements of the view
+// type), batched `howmany` times at distance `dist`.
+static View axis_view(void* ptr, const std::vector<long long>& D, int a, long long howmany, long long dist) {
+    View v;
+    v.ptr = ptr;
+    long long inner = 1, outer = 1;
+    for (size_t i = a + 1; i < D.size(); ++i) inner *= D[i];
+    for (int i = 0; i < a; ++i) outer *= D[i];
+    v.estride = inner;
+    int nb = 0;
+    if (inner > 1) { v.cnt[nb] = inner; v.str[nb] = 1; ++nb; }
+    if (outer > 1) { v.cnt[nb] = outer; v.str[nb] = D[a] * inner; ++nb; }
+    if (howmany > 1) { v.cnt[nb] = howmany; v.str[nb] = dist; ++nb; }
+    v.nb = nb;
+    return v;
+}
+
+static OpSpec real_op(int kind, int n) {
+    OpSpec op;
+    op.N = n;
+    op.logN = ilog2(n);
+    switch (kind) {
+    case K_REALDFT: op.ld = LD_R2C; op.st = ST_R; op.paired = true; break;
+    case K_INVREALDFT: op.ld = LD_IR; op.st = ST_C2R; op.conj_out = 1; break;
+    case K_DCT2: op.ld = LD_T2; op.st = ST_T2; op.paired = true; break;
+    case K_DST2: op.ld = LD_T2; op.st = ST_T2; op.paired = true; op.dst = 1; break;
+    case K_DCT3: op.ld = LD_T3; op.st = ST_T3; break;
+    case K_DST3: op.ld = LD_T3; op.st = ST_T3; op.dst = 1; break;
+    case K_DCT4: op.ld = LD_T4; op.st = ST_T4; break;
+    case K_DST4: op.ld = LD_T4; op.st = ST_T4; op.dst = 1; break;
+    }
+    return op;
+}
+
+// Size-1 factor of the real families (the reference's N = 1 cases).
+static double tiny_factor(int kind) {
+    switch (kind) {
+    case K_DCT2: case K_DST2: return 2.0;
+    case K_DCT4: case K_DST4: return 1.41421356237309504880;
+    default: return 1.0;
+    }
+}
+
+// One real-family 1-D transform along axis `a` (src -> dst views).
+static bool run_real_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisPlan& ax, int kind, const View& src,
+                          const View& dst, int vjp, double unit_factor, cudaStream_t s) {
+    if (ax.n == 1) {
+        // every line is one element: y = factor * x (complex in/out for the realdft pair)
+        long long lines = src.lines();
+        if (src.nb > 1 || dst.nb > 1) {
+            // N-D size-1 axes are skipped by the caller; only 1-D batches reach here
+            set_error(6, "size-1 axis inside a multi-dimensional real transform");
+            return false;
+        }
+        long long idist = src.nb ? src.str[0] : 1, odist = dst.nb ? dst.str[0] : 1;
+        int in_c = kind == K_INVREALDFT, out_c = kind == K_REALDFT;
+        return launch_tiny((const real_t*)src.ptr, (real_t*)dst.ptr, lines, 1, idist, odist, in_c, out_c, unit_factor, s);
+    }
+    OpSpec op = real_op(kind, ax.n);
+    op.vjp = vjp;
+    return run_pow2_axis(p, c, ax, src, dst, op, s);
+}
+
+// Adjoint pipelines: the transposed transform of each family (complex data
+// treated as pairs of reals).  dft <-> unnormalized inverse; realdft <->
+// invrealdft with interior-bin weights; DCT-2 <-> DCT-3 and DST-2 <-> DST-3
+// with the first / last coefficient weighted; DCT-4 and DST-4 are symmetric.
+static int adjoint_kind(int kind) {
+    switch (kind) {
+    case K_REALDFT: return K_INVREALDFT;
+    case K_INVREALDFT: return K_REALDFT;
+    case K_DCT2: return K_DCT3;
+    case K_DST2: return K_DST3;
+    case K_DCT3: return K_DCT2;
+    case K_DST3: return K_DST2;
+    default: return kind;
+    }
+}
+
+int plan_execute(notorious_fft_plan* p, int okind, const void* in, void* out, long long howmany, long long idist,
+                 long long odist, cudaStream_t stream, int vjp) {
+    const int kind = vjp ? adjoint_kind(okind) : okind;
+    const double unit_factor = tiny_factor(okind);
+    DeviceCtx* c = device_ctx(p->device);
+    if (!c) return last_error();
+    const int d = (int)p->dims.size();
+    std::vector<long long> D(p->dims.begin(), p->dims.end());
+    if (howmany < 1) return 0;
+    const int fam = family_of(kind);
+    if (fam != p->family) {
+        set_error(1, "transform kind %d does not match the aux family %d", kind, p->family);
+        return 1;
+    }
+    bool ok = true;
+    if (fam == FAM_DFT) {
+        // forward / inverse direction; the Bluestein 1/n factor belongs to invdft
+        // and is kept by the adjoint of invdft (a forward pass scaled by 1/n)
+        const int inverse = (okind == K_INVDFT) != (vjp != 0);
+        const bool scale_blue = okind == K_INVDFT;
+        for (int step = 0; step < d && ok; ++step) {
+            int a = d - 1 - step;
+            const void* sp = step == 0 ? in : out;
+            View src = axis_view((void*)sp, D, a, howmany, step == 0 ? idist : odist);
+            View dst = axis_view(out, D, a, howmany, odist);
+            const AxisPlan& ax = p->axes[a];
+            if (ax.n == 1) {
+                if (step == 0 && in != out) {
+                    // identity axis: the data still has to reach `out`
+                    if (d == 1) {
+                        ok = cuda_ok(cudaMemcpy2DAsync(out, (size_t)odist * sizeof(cplx_t), in, (size_t)idist * sizeof(cplx_t),
+                                                       sizeof(cplx_t), (size_t)howmany, cudaMemcpyDeviceToDevice, stream),
+                                     "copy of size-1 transform");
+                    } else {
+                        OpSpec op;
+                        AxisPlan one;
+                        one.fft_contig = make_schedule(0, false);
+                        one.fft_strided = make_schedule(0, true);
+                        ok = run_pow2_axis(p, c, one, src, dst, op, stream);
+                    }
+                }
+                continue;
+            }
+            if (ax.pow2) {
+                OpSpec op;
+                op.conj_in = op.conj_out = inverse;
+                ok = run_pow2_axis(p, c, ax, src, dst, op, stream);
+            } else {
+                ok = run_bluestein_axis(p, c, ax, src, dst, inverse, scale_blue ? 1.0 / (double)ax.n : 1.0, stream);
+            }
+        }
+    } else if (fam == FAM_REAL) {
+        std::vector<long long> H = D;
+        H.back() = D.back() / 2 + 1;
+        if (kind == K_REALDFT) {
+            View src = axis_view((void*)in, D, d - 1, howmany, idist);
+            View dst = axis_view(out, H, d - 1, howmany, odist);
+            ok = run_real_axis(p, c, p->axes[d - 1], kind, src, dst, vjp, unit_factor, stream);
+            for (int a = d - 2; a >= 0 && ok; --a) {
+                if (p->axes[a].n == 1) continue;
+                View v = axis_view(out, H, a, howmany, odist);
+                OpSpec op;
+                AxisPlan ax = p->axes[a];
+                ok = run_pow2_axis(p, c, ax, v, v, op, stream);
+            }
+        } else {
+            // complex inverse DFTs along the leading axes into a temporary (the
+            // caller's input is left untouched), then invrealdft along the last axis
+            const void* src_ptr = in;
+            long long sdist = idist;
+            if (d > 1) {
+                long long per = prod(p->dims, 0, d - 1) * H.back();
+                size_t bytes = (size_t)per * (size_t)howmany * sizeof(cplx_t);
+                if (p->nd_tmp == nullptr || p->nd_tmp_bytes < bytes) {
+                    if (p->nd_tmp) cudaFree(p->nd_tmp);
+                    p->nd_tmp = nullptr;
+                    p->nd_tmp_bytes = 0;
+                    if (!cuda_ok(cudaMalloc(&p->nd_tmp, bytes), "cudaMalloc(N-D temporary)")) return last_error();
+                    p->nd_tmp_bytes = bytes;
+                }
+                bool firstc = true;
+                for (int a = d - 2; a >= 0 && ok; --a) {
+                    if (p->axes[a].n == 1) continue;
+                    View vs = axis_view(firstc ? (void*)in : p->nd_tmp, H, a, howmany, firstc ? idist : per);
+                    View vd = axis_view(p->nd_tmp, H, a, howmany, per);
+                    OpSpec op;
+                    op.conj_in = op.conj_out = 1;
+                    ok = run_pow2_axis(p, c, p->axes[a], vs, vd, op, stream);
+                    firstc = false;
+                }
+                if (!firstc) {
+                    src_ptr = p->nd_tmp;
+                    sdist = per;
+                }
+            }
+            View src = axis_view((void*)src_ptr, H, d - 1, howmany, sdist);
+            View dst = axis_view(out, D, d - 1, howmany, odist);
+            ok = ok && run_real_axis(p, c, p->axes[d - 1], kind, src, dst, vjp, unit_factor, stream);
+        }
+    } else {
+        // real-to-real families: the reference transforms axis k only while the
+        // product of the axes after it exceeds 1 (src/07_legacy.h:822-861), so
+        // trailing length-1 axes are skipped; length-1 axes before that scale by
+        // the 1-D N=1 factor.
+        int last = 0;
+        for (int i = 0; i < d; ++i)
+            if (p->dims[i] != 1) last = i;
+        if (d == 1) {
+            View src = axis_view((void*)in, D, 0, howmany, idist);
+            View dst = axis_view(out, D, 0, howmany, odist);
+            ok = run_real_axis(p, c, p->axes[0], kind, src, dst, vjp, unit_factor, stream);
+        } else {
+            const long long total = prod(p->dims, 0, d);
+            bool first = true;
+            for (int a = last; a >= 0 && ok; --a) {
+                const void* sp = first ? in : out;
+                long long sdist = first ? idist : odist;
+                if (p->axes[a].n == 1) {
+                    ok = launch_tiny((const real_t*)sp, (real_t*)out, howmany, total, sdist, odist, 0, 0,
+                                     unit_factor, stream);
+                } else {
+                    View src = axis_view((void*)sp, D, a, howmany, sdist);
+                    View dst = axis_view(out, D, a, howmany, odist);
+                    ok = run_real_axis(p, c, p->axes[a], kind, src, dst, vjp, unit_factor, stream);
+                }
+                first = false;
+            }
+        }
+    }
+    if (!ok) return last_error() ? last_error() : 4;
+    return 0;
+}
+
+}  // namespace nfft

@@ -1,0 +1,318 @@
+// nfft_emu.cu -- TEST INFRASTRUCTURE ONLY: a CPU emulation build of the
+// library's host logic, used by the CPU test suite (tests/test_emulator.py).
+//
+// It compiles the library's planner and C ABI (notorious-fft_b200/csrc/
+// nfft_plan.cu, nfft_api.cu) against an emulated CUDA runtime (host memory,
+// synchronous copies) and replaces every kernel launch with a host loop that
+// runs the kernel's own per-thread phase functions (nfft_pass.cuh: line_setup,
+// load_slot, substage_read/write, mid_slot, store_slot, paired_slot,
+// unpack_item) for every thread of every tile.  Every global and shared
+// memory access is bounds-checked against live allocations; a violation
+// aborts the process with the offending address.  Fresh allocations are
+// filled with NaN so reads of unwritten scratch show up in the results.
+//
+// This build is never shipped: the product libraries have no CPU path.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <vector>
+
+// ---------------------------------------------------------------------------
+// emulated runtime
+// ---------------------------------------------------------------------------
+namespace emu {
+static std::mutex mu;
+static std::map<uintptr_t, size_t> allocs;   // base -> bytes
+static std::map<uintptr_t, size_t> host_ok;  // user host buffers registered by the tests
+static long long n_checks = 0;
+
+static bool inside(const std::map<uintptr_t, size_t>& m, uintptr_t p, size_t b) {
+    auto it = m.upper_bound(p);
+    if (it == m.begin()) return false;
+    --it;
+    return p >= it->first && p + b <= it->first + it->second;
+}
+
+cudaError_t Malloc(void** p, size_t bytes) {
+    void* q = malloc(bytes ? bytes : 1);
+    if (!q) return cudaErrorMemoryAllocation;
+    // NaN fill: scratch read before it is written poisons the result
+    double nan = NAN;
+    for (size_t i = 0; i + sizeof(double) <= bytes; i += sizeof(double)) memcpy((char*)q + i, &nan, sizeof(double));
+    std::lock_guard<std::mutex> lk(mu);
+    allocs[(uintptr_t)q] = bytes;
+    *p = q;
+    return cudaSuccess;
+}
+cudaError_t Free(void* p) {
+    if (!p) return cudaSuccess;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = allocs.find((uintptr_t)p);
+    if (it == allocs.end()) {
+        fprintf(stderr, "nfft_emu: cudaFree of unknown pointer %p\n", p);
+        abort();
+    }
+    allocs.erase(it);
+    free(p);
+    return cudaSuccess;
+}
+static bool is_dev(const void* p, size_t b) {
+    std::lock_guard<std::mutex> lk(mu);
+    return inside(allocs, (uintptr_t)p, b);
+}
+static void check_range(const void* p, size_t b, const char* what) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!inside(allocs, (uintptr_t)p, b) && !inside(host_ok, (uintptr_t)p, b)) {
+        fprintf(stderr, "nfft_emu: %s out of bounds: %p + %zu\n", what, p, b);
+        abort();
+    }
+}
+cudaError_t MemcpyAsync(void* d, const void* s, size_t b, cudaMemcpyKind, cudaStream_t = 0) {
+    check_range(d, b, "memcpy dst");
+    check_range(s, b, "memcpy src");
+    memmove(d, s, b);
+    return cudaSuccess;
+}
+cudaError_t Memcpy2DAsync(void* d, size_t dp, const void* s, size_t sp, size_t w, size_t h, cudaMemcpyKind k,
+                          cudaStream_t st = 0) {
+    for (size_t r = 0; r < h; ++r) MemcpyAsync((char*)d + r * dp, (const char*)s + r * sp, w, k, st);
+    return cudaSuccess;
+}
+cudaError_t Ok(...) { return cudaSuccess; }
+cudaError_t GetDevice(int* d) {
+    *d = 0;
+    return cudaSuccess;
+}
+cudaError_t GetDeviceProperties(cudaDeviceProp* p, int) {
+    memset(p, 0, sizeof *p);
+    strcpy(p->name, "emulated sm_100");
+    p->major = 10;
+    p->minor = 0;
+    p->multiProcessorCount = 148;
+    p->l2CacheSize = 126 << 20;
+    return cudaSuccess;
+}
+cudaError_t PointerGetAttributes(cudaPointerAttributes* a, const void* p) {
+    memset(a, 0, sizeof *a);
+    a->type = is_dev(p, 1) ? cudaMemoryTypeDevice : cudaMemoryTypeUnregistered;
+    return cudaSuccess;
+}
+const char* ErrorString(cudaError_t) { return "emulated CUDA error"; }
+}  // namespace emu
+
+static int g_smem_elems = 0;
+__host__ __device__ void nfft_emu_check(const void* p, size_t bytes, int write) {
+#ifndef __CUDA_ARCH__
+    emu::n_checks++;
+    emu::check_range(p, bytes, write ? "global store" : "global load");
+#endif
+}
+namespace nfft {
+__host__ __device__ void nfft_emu_smem_check(int idx) {
+#ifndef __CUDA_ARCH__
+    if (idx < 0 || idx >= g_smem_elems) {
+        fprintf(stderr, "nfft_emu: shared memory index %d outside [0, %d)\n", idx, g_smem_elems);
+        abort();
+    }
+#endif
+}
+}  // namespace nfft
+
+#define cudaMalloc(p, b) emu::Malloc((void**)(p), (b))
+#define cudaFree emu::Free
+#define cudaMemcpyAsync emu::MemcpyAsync
+#define cudaMemcpy2DAsync emu::Memcpy2DAsync
+#define cudaStreamSynchronize(s) emu::Ok()
+#define cudaDeviceSynchronize() emu::Ok()
+#define cudaSetDevice(d) emu::Ok()
+#define cudaGetDevice emu::GetDevice
+#undef cudaGetDeviceProperties
+#define cudaGetDeviceProperties emu::GetDeviceProperties
+#define cudaPointerGetAttributes emu::PointerGetAttributes
+#define cudaGetLastError() emu::Ok()
+#define cudaGetErrorString emu::ErrorString
+
+#include "../../notorious-fft_b200/csrc/nfft_plan.cu"
+#include "../../notorious-fft_b200/csrc/nfft_api.cu"
+
+// ---------------------------------------------------------------------------
+// emulated launches: the kernels' phase functions for every thread
+// ---------------------------------------------------------------------------
+namespace nfft {
+
+template <int LOG_TILE, int LOAD, int STORE>
+static void emu_pass(const PassArgs& a, long long ntiles) {
+    using T = real_t;
+    using V = C2<T>;
+    constexpr int THREADS = (1 << LOG_TILE) / 16;
+    const TwTables<T>* tw = (const TwTables<T>*)a.tw;
+    const int logE = a.logR + a.logJ, J = 1 << a.logJ, E = 1 << logE;
+    g_smem_elems = (int)pass_smem_elems<T>(LOG_TILE);
+    std::vector<V> sm(g_smem_elems);
+    std::vector<long long> lin(MAX_J), lout(MAX_J), lj(MAX_J);
+    std::vector<V> regs((size_t)THREADS * 16);
+    TileLines tl{lin.data(), lout.data(), lj.data()};
+    if (J > MAX_J || E > (1 << LOG_TILE)) {
+        fprintf(stderr, "nfft_emu: tile of %d lines x 2^%d exceeds the kernel limits\n", J, a.logR);
+        abort();
+    }
+    auto fft = [&]() {
+        int lns = 0;
+        for (int s = 0; s < a.nsub; ++s) {
+            int lr = a.sublog[s];
+            for (int t = 0; t < THREADS; ++t) {
+                V* v = &regs[(size_t)t * 16];
+                switch (lr) {
+                case 4: substage_read<T, THREADS, 16, 4>(sm.data(), v, a.logR, logE, t); break;
+                case 3: substage_read<T, THREADS, 8, 3>(sm.data(), v, a.logR, logE, t); break;
+                case 2: substage_read<T, THREADS, 4, 2>(sm.data(), v, a.logR, logE, t); break;
+                default: substage_read<T, THREADS, 2, 1>(sm.data(), v, a.logR, logE, t); break;
+                }
+            }
+            for (int t = 0; t < THREADS; ++t) {
+                V* v = &regs[(size_t)t * 16];
+                switch (lr) {
+                case 4: substage_write<T, THREADS, 16, 4>(sm.data(), v, tw, a.logR, logE, lns, t); break;
+                case 3: substage_write<T, THREADS, 8, 3>(sm.data(), v, tw, a.logR, logE, lns, t); break;
+                case 2: substage_write<T, THREADS, 4, 2>(sm.data(), v, tw, a.logR, logE, lns, t); break;
+                default: substage_write<T, THREADS, 2, 1>(sm.data(), v, tw, a.logR, logE, lns, t); break;
+                }
+            }
+            lns += lr;
+        }
+    };
+    for (long long tile = 0; tile < ntiles; ++tile) {
+        const long long line0 = tile << a.logJ;
+        if (line0 >= a.nlines) continue;
+        for (auto& x : sm) x = mkc((T)NAN, (T)NAN);
+        for (int l = 0; l < J; ++l) line_setup(a, line0 + l, l, tl);
+        for (int t = 0; t < THREADS; ++t)
+            for (int it = 0; it < 16; ++it) {
+                int e = t + it * THREADS;
+                if (e >= E) break;
+                load_slot<T, LOAD>(a, tw, sm.data(), tl, e);
+            }
+        fft();
+        if (a.mid) {
+            for (int e = 0; e < E; ++e) mid_slot<T>(a, sm.data(), tl, e);
+            fft();
+        }
+        if constexpr (STORE == ST_R || STORE == ST_T2) {
+            const int items = paired_items(a);
+            for (int w = 0; w < items; ++w) paired_slot<T, STORE>(a, tw, sm.data(), tl, w);
+        } else {
+            for (int e = 0; e < E; ++e) store_slot<T, STORE>(a, tw, sm.data(), tl, e);
+        }
+    }
+}
+
+using EmuFn = void (*)(const PassArgs&, long long);
+
+#define NFFT_PAIRS(X) \
+    X(LD_C, ST_C) X(LD_C, ST_R) X(LD_C, ST_T2) X(LD_C, ST_T3) X(LD_C, ST_T4) X(LD_C, ST_BLUE) X(LD_T2, ST_C) \
+    X(LD_T2, ST_T2) X(LD_T3, ST_C) X(LD_T3, ST_T3) X(LD_IR, ST_C) X(LD_T4, ST_C) X(LD_T4, ST_T4)          \
+    X(LD_BLUE, ST_C) X(LD_BLUE, ST_BLUE) X(LD_R2C, ST_C) X(LD_R2C, ST_R) X(LD_C, ST_C2R) X(LD_IR, ST_C2R)
+
+static long long g_launches = 0;
+
+bool launch_pass(const PassArgs& a, int ld, int st, int log_tile, long long ntiles, cudaStream_t) {
+    static EmuFn t12[7][7] = {}, t13[7][7] = {};
+    static bool filled = false;
+    if (!filled) {
+#define X(L, S) t12[L][S] = emu_pass<12, L, S>; t13[L][S] = emu_pass<13, L, S>;
+        NFFT_PAIRS(X)
+#undef X
+        filled = true;
+    }
+    EmuFn f = (log_tile == 13 ? t13 : t12)[ld][st];
+    if (!f || (log_tile != 12 && log_tile != 13)) {
+        set_error(6, "no pass kernel for load op %d / store op %d / tile %d", ld, st, log_tile);
+        return false;
+    }
+    g_launches++;
+    f(a, ntiles);
+    return true;
+}
+
+bool launch_unpack(const PassArgs& a, int st, const cplx_t* Z, long long zdist, long long nlines, cudaStream_t) {
+    const TwTables<real_t>* tw = (const TwTables<real_t>*)a.tw;
+    long long M = a.N / 2, per = M >= 2 ? M / 2 : 1;
+    g_launches++;
+    for (long long w = 0; w < per * nlines; ++w) {
+        if (st == ST_R) unpack_item<real_t, ST_R>(a, tw, Z, zdist, w);
+        else unpack_item<real_t, ST_T2>(a, tw, Z, zdist, w);
+    }
+    return true;
+}
+
+bool launch_tiny(const real_t* x, real_t* y, long long howmany, long long inner, long long idist, long long odist,
+                 int in_cplx, int out_cplx, double factor, cudaStream_t) {
+    g_launches++;
+    for (long long b = 0; b < howmany; ++b)
+        for (long long i = 0; i < inner; ++i) {
+            real_t v = NFFT_GLD(&x[(b * idist + i) * (in_cplx ? 2 : 1)]);
+            real_t r = (real_t)(factor * (double)v);
+            if (out_cplx) {
+                NFFT_GST(&y[(b * odist + i) * 2], r);
+                NFFT_GST(&y[(b * odist + i) * 2 + 1], (real_t)0);
+            } else {
+                NFFT_GST(&y[b * odist + i], r);
+            }
+        }
+    return true;
+}
+
+bool launch_init_tables(TwTables<real_t>* tw, cudaStream_t) {
+    for (int level = 0; level < 3; ++level)
+        for (int m = 0; m < TW_SIZE; ++m) {
+            long double frac = ldexpl((long double)m, 1 - TW_BITS * (level + 1));
+            long double ang = 3.141592653589793238462643383279502884L * frac;
+            tw->t[level][m] = mkc((real_t)cosl(ang), (real_t)-sinl(ang));
+        }
+    return true;
+}
+
+bool launch_chirp(cplx_t* chirp, cplx_t* bwrap, long long n, long long M, cudaStream_t) {
+    for (long long k = 0; k < M; ++k) {
+        if (k < n) {
+            unsigned long long r = ((unsigned long long)k * (unsigned long long)k) % (unsigned long long)(2 * n);
+            long double ang = 3.141592653589793238462643383279502884L * (long double)r / (long double)n;
+            real_t c = (real_t)cosl(ang), s = (real_t)sinl(ang);
+            chirp[k] = mkc(c, (real_t)-s);
+            bwrap[k] = mkc(c, s);
+            if (k > 0) bwrap[M - k] = mkc(c, s);
+        } else if (k <= M - n) {
+            bwrap[k] = mkc((real_t)0, (real_t)0);
+        }
+    }
+    return true;
+}
+
+bool set_kernel_attributes() { return true; }
+long long launch_count() { return g_launches; }
+
+}  // namespace nfft
+
+extern "C" {
+// Test hooks: "device" memory of the emulator, launch counter.
+void* nfft_emu_malloc(size_t bytes) {
+    void* p = nullptr;
+    return emu::Malloc(&p, bytes) == cudaSuccess ? p : nullptr;
+}
+void nfft_emu_free(void* p) { emu::Free(p); }
+void nfft_emu_register_host(void* p, size_t bytes) {
+    std::lock_guard<std::mutex> lk(emu::mu);
+    emu::host_ok[(uintptr_t)p] = bytes;
+}
+void nfft_emu_unregister_host(void* p) {
+    std::lock_guard<std::mutex> lk(emu::mu);
+    emu::host_ok.erase((uintptr_t)p);
+}
+long long nfft_emu_launches(void) { return nfft::g_launches; }
+long long nfft_emu_checks(void) { return emu::n_checks; }
+}
