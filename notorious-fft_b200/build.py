@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import argparse
 import concurrent.futures as cf
+import hashlib
 import os
 import shutil
 import subprocess
@@ -25,7 +26,7 @@ LIB = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu"]
+SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu"] + [f"nfft_lean_s{k}.cu" for k in range(8)]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 PRECISIONS = {
     "d": ("libnotorious_fft.so", ["-DNFFT_REAL=double"]),
@@ -40,26 +41,57 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _newer(target: str, deps: list[str]) -> bool:
-    if not os.path.exists(target):
+def _digest(deps: list[str], cmd: list[str]) -> str:
+    h = hashlib.sha256(" ".join(cmd).encode())
+    for d in sorted(deps):
+        with open(d, "rb") as f:
+            h.update(d.encode())
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def _fresh(target: str, deps: list[str], cmd: list[str]) -> bool:
+    """True when target exists and was built from exactly these inputs."""
+    stamp = target + ".stamp"
+    if not (os.path.exists(target) and os.path.exists(stamp)):
         return False
-    t = os.path.getmtime(target)
-    return all(os.path.getmtime(d) <= t for d in deps)
+    with open(stamp) as f:
+        return f.read().strip() == _digest(deps, cmd)
 
 
-def _headers() -> list[str]:
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    hs.append(os.path.join(INCLUDE, "notorious_fft.h"))
-    return hs
+def _stamp(target: str, deps: list[str], cmd: list[str]) -> None:
+    with open(target + ".stamp", "w") as f:
+        f.write(_digest(deps, cmd))
+
+
+def _includes(path: str, seen: set) -> None:
+    """Local headers included by `path`, transitively."""
+    import re
+    with open(path) as f:
+        for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', f.read(), flags=re.M):
+            for base in (os.path.dirname(path), CSRC, INCLUDE):
+                cand = os.path.normpath(os.path.join(base, name))
+                if os.path.exists(cand):
+                    if cand not in seen:
+                        seen.add(cand)
+                        _includes(cand, seen)
+                    break
+
+
+def _headers(src: str) -> list[str]:
+    seen: set = set()
+    _includes(os.path.join(CSRC, src), seen)
+    return sorted(seen)
 
 
 def compile_one(src: str, prec: str, extra: list[str], verbose_ptxas: bool) -> str:
     obj = os.path.join(BUILD, f"{os.path.splitext(src)[0]}_{prec}.o")
-    deps = [os.path.join(CSRC, src)] + _headers()
-    if _newer(obj, deps) and not verbose_ptxas:
-        return obj
+    deps = [os.path.join(CSRC, src)] + _headers(src)
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
            "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+    if _fresh(obj, deps, cmd) and not verbose_ptxas:
+        return obj
+    digest = _digest(deps, cmd)   # inputs as compiled (edits during the compile force a rebuild next time)
     if verbose_ptxas:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -67,10 +99,12 @@ def compile_one(src: str, prec: str, extra: list[str], verbose_ptxas: bool) -> s
         raise RuntimeError(f"nvcc failed for {src} ({prec}):\n{r.stderr}")
     if verbose_ptxas:
         sys.stderr.write(r.stderr)
+    with open(obj + ".stamp", "w") as f:
+        f.write(digest)
     return obj
 
 
-def build(only: str | None = None, jobs: int = 6, verbose_ptxas: bool = False) -> list[str]:
+def build(only: str | None = None, jobs: int = 8, verbose_ptxas: bool = False) -> list[str]:
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(BUILD, exist_ok=True)
     precs = [only] if only else list(PRECISIONS)
@@ -85,12 +119,14 @@ def build(only: str | None = None, jobs: int = 6, verbose_ptxas: bool = False) -
         name = PRECISIONS[p][0]
         out = os.path.join(LIB, name)
         pobjs = [objs[(p, s)] for s in SOURCES]
-        if not _newer(out, pobjs):
-            cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-Xlinker", "-Bsymbolic", "-o", out, *pobjs,
-                   "-lcudart_static", "-ldl", "-lrt", "-lpthread"]
+        cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-Xlinker", "-Bsymbolic", "-Xlinker", "--no-undefined",
+               "-o", out, *pobjs, "-lcudart_static", "-ldl", "-lrt", "-lpthread"]
+        deps = pobjs + [o + ".stamp" for o in pobjs]
+        if not _fresh(out, deps, cmd):
             r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise RuntimeError(f"link failed for {name}:\n{r.stderr}")
+            _stamp(out, deps, cmd)
         outs.append(out)
     return outs
 
@@ -99,7 +135,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", choices=sorted(PRECISIONS))
     ap.add_argument("--ptxas", action="store_true", help="print -Xptxas -v resource usage")
-    ap.add_argument("-j", type=int, default=6)
+    ap.add_argument("-j", type=int, default=8)
     args = ap.parse_args()
     for o in build(args.only, args.j, args.ptxas):
         print(o)

@@ -46,6 +46,65 @@ template <typename V> NFFT_HD V mul_mi(V a) { return mkc(a.y, -a.x); }
 template <typename V, typename S> NFFT_HD V cscale(V a, S s) { return mkc(a.x * s, a.y * s); }
 
 // ---------------------------------------------------------------------------
+// Global accesses with L2 policy.  hint 0: default; 1: streaming (user data
+// read or written once: evict first); 2: inter-pass scratch (stores kept in L2
+// with evict_last priority; the last read is followed by discard_l2).
+// ---------------------------------------------------------------------------
+template <typename V>
+NFFT_HD V gload(const V* p, int hint) {
+#if defined(__CUDA_ARCH__)
+    if (hint == 1 || hint == 2) return __ldcs(p);
+    return *p;
+#else
+    (void)hint;
+    return NFFT_GLD(p);
+#endif
+}
+
+NFFT_HD void gstore(double2* p, double2 v, int hint) {
+#if defined(__CUDA_ARCH__)
+    if (hint == 1) { __stcs(p, v); return; }
+    if (hint == 2) {
+        uint64_t pol;
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+        asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y), "l"(pol)
+                     : "memory");
+        return;
+    }
+    *p = v;
+#else
+    (void)hint;
+    NFFT_GST(p, v);
+#endif
+}
+
+NFFT_HD void gstore(float2* p, float2 v, int hint) {
+#if defined(__CUDA_ARCH__)
+    if (hint == 1) { __stcs(p, v); return; }
+    if (hint == 2) {
+        uint64_t pol;
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+        asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol)
+                     : "memory");
+        return;
+    }
+    *p = v;
+#else
+    (void)hint;
+    NFFT_GST(p, v);
+#endif
+}
+
+// Drop a 128-byte line from L2 without writing it back (dead scratch data).
+NFFT_HD void discard_l2(const void* p) {
+#if defined(__CUDA_ARCH__)
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+#else
+    (void)p;
+#endif
+}
+
+// ---------------------------------------------------------------------------
 // Twiddle tables.  W_P^q = exp(-2 pi i q / P) for any power of two P <= 2^36
 // is assembled from three 4096-entry tables that split a 36-bit fraction of a
 // turn into 12-bit digits:  u = q * 2^(36 - log2 P),

@@ -145,4 +145,30 @@ bool launch_chirp(cplx_t* chirp, cplx_t* bwrap, long long n, long long M, cudaSt
 bool set_kernel_attributes();
 long long launch_count();
 
+// Specialized pass kernels (nfft_lean.cuh), registered by the slice files.
+constexpr int NFFT_LEAN_SLICES = 8;
+inline unsigned lean_key(int logR, int logT, int ci, int co, int ld, int st) {
+    return (unsigned)logR | ((unsigned)logT << 5) | ((unsigned)ci << 10) | ((unsigned)co << 11) | ((unsigned)ld << 12) |
+           ((unsigned)st << 16);
+}
+struct LeanEntry {
+    const void* fn = nullptr;
+    size_t smem = 0;
+    int threads = 0;
+};
+struct LeanRegistry {
+    std::vector<std::pair<unsigned, LeanEntry>> entries;
+    void add(unsigned key, const void* fn, size_t smem, int threads) { entries.push_back({key, LeanEntry{fn, smem, threads}}); }
+    const LeanEntry* find(unsigned key) const {
+        for (auto& e : entries)
+            if (e.first == key) return &e.second;
+        return nullptr;
+    }
+};
+const LeanRegistry& lean_registry();
+// Launch the specialized kernel for this pass shape, or return false with no
+// error set when none is instantiated (the caller then uses pass_kernel).
+bool lean_available(int logR, int logT, int ci, int co, int ld, int st);
+bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, long long ntiles, cudaStream_t s);
+
 }  // namespace nfft

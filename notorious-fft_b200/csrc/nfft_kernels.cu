@@ -53,7 +53,57 @@ static PassFn pass_table(int log_tile, int ld, int st) {
     return log_tile == 13 ? t13[ld][st] : (log_tile == 12 ? t12[ld][st] : nullptr);
 }
 
+void lean_register_slice_0(LeanRegistry&);
+void lean_register_slice_1(LeanRegistry&);
+void lean_register_slice_2(LeanRegistry&);
+void lean_register_slice_3(LeanRegistry&);
+void lean_register_slice_4(LeanRegistry&);
+void lean_register_slice_5(LeanRegistry&);
+void lean_register_slice_6(LeanRegistry&);
+void lean_register_slice_7(LeanRegistry&);
+
+const LeanRegistry& lean_registry() {
+    static LeanRegistry reg = [] {
+        LeanRegistry r;
+        lean_register_slice_0(r);
+        lean_register_slice_1(r);
+        lean_register_slice_2(r);
+        lean_register_slice_3(r);
+        lean_register_slice_4(r);
+        lean_register_slice_5(r);
+        lean_register_slice_6(r);
+        lean_register_slice_7(r);
+        return r;
+    }();
+    return reg;
+}
+
+bool lean_available(int logR, int logT, int ci, int co, int ld, int st) {
+    return lean_registry().find(lean_key(logR, logT, ci, co, ld, st)) != nullptr;
+}
+
+bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, long long ntiles, cudaStream_t s) {
+    const LeanEntry* e = lean_registry().find(lean_key(a.logR, logT, ci, co, ld, st));
+    if (!e) {
+        set_error(6, "no specialized pass kernel for radix 2^%d", a.logR);
+        return false;
+    }
+    if (ntiles <= 0) return true;
+    dim3 grid;
+    if (ntiles <= 0x7fffffffll) grid = dim3((unsigned)ntiles, 1, 1);
+    else grid = dim3(0x7fffffffu, (unsigned)((ntiles + 0x7fffffffll - 1) / 0x7fffffffll), 1);
+    void* args[] = {(void*)&a};
+    cudaError_t err = cudaLaunchKernel(e->fn, grid, dim3(e->threads, 1, 1), args, e->smem, s);
+    g_launches++;
+    return cuda_ok(err, "specialized pass kernel launch");
+}
+
 bool set_kernel_attributes() {
+    for (auto& kv : lean_registry().entries) {
+        if (!cuda_ok(cudaFuncSetAttribute(kv.second.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kv.second.smem),
+                     "cudaFuncSetAttribute(lean pass)"))
+            return false;
+    }
     for (int lt = 12; lt <= 13; ++lt) {
         size_t smem = pass_smem_bytes<real_t>(lt);
         for (int ld = 0; ld < NLOAD; ++ld)

@@ -1,0 +1,348 @@
+// nfft_lean.cuh -- the specialized pass kernel (hot path).
+//
+// Same Stockham pass semantics as pass_kernel (nfft_pass.cuh), with the pass
+// radix R = 2^LOGR and the tile shape fixed at compile time:
+//  * the first sub-stage is radix 16 and reads its 16 points per thread
+//    straight from global memory (no shared-memory staging), with the pass
+//    pre-twiddle W_{Ns R}^{r k} generated per line from two table roots and
+//    a depth-4 product tree;
+//  * middle sub-stages exchange through shared memory;
+//  * the last sub-stage writes its outputs straight to global memory, except
+//    for the paired real operators, which need whole lines in shared memory.
+// Thread-to-butterfly mappings are chosen per sub-stage so that global
+// accesses coalesce: "column" mode walks consecutive lines (J adjacent
+// Stockham lines or a unit-stride batch dim), "row" mode walks along a line.
+// Column tiles are stored [r][line] with a pitch of J+1 points, row tiles
+// [line][r] with one pad point every 16, which keeps both mappings free of
+// shared-memory bank conflicts.
+#pragma once
+
+#include "nfft_pass.cuh"
+
+namespace nfft {
+
+// Sub-stage radices (log2) of a pass of radix 2^LOGR: radix 16 first.
+template <int LOGR> struct LeanSched;
+template <> struct LeanSched<4> { static constexpr int n = 1; static constexpr int lr[4] = {4, 0, 0, 0}; };
+template <> struct LeanSched<5> { static constexpr int n = 2; static constexpr int lr[4] = {4, 1, 0, 0}; };
+template <> struct LeanSched<6> { static constexpr int n = 2; static constexpr int lr[4] = {4, 2, 0, 0}; };
+template <> struct LeanSched<7> { static constexpr int n = 2; static constexpr int lr[4] = {4, 3, 0, 0}; };
+template <> struct LeanSched<8> { static constexpr int n = 2; static constexpr int lr[4] = {4, 4, 0, 0}; };
+template <> struct LeanSched<9> { static constexpr int n = 3; static constexpr int lr[4] = {4, 3, 2, 0}; };
+template <> struct LeanSched<10> { static constexpr int n = 3; static constexpr int lr[4] = {4, 4, 2, 0}; };
+template <> struct LeanSched<11> { static constexpr int n = 3; static constexpr int lr[4] = {4, 4, 3, 0}; };
+template <> struct LeanSched<12> { static constexpr int n = 3; static constexpr int lr[4] = {4, 4, 4, 0}; };
+template <> struct LeanSched<13> { static constexpr int n = 4; static constexpr int lr[4] = {4, 4, 3, 2}; };
+
+// Shared-memory index of point r of tile line l.
+template <bool COL, int LOGR, int LOGJ>
+NFFT_HD int lean_idx(int l, int r) {
+    if constexpr (COL) return r * ((1 << LOGJ) + 1) + l;
+    else return spad((l << LOGR) + r);
+}
+template <bool COL, int LOGR, int LOGJ> constexpr int lean_smem_elems() {
+    return COL ? (1 << LOGR) * ((1 << LOGJ) + 1) : ((1 << (LOGR + LOGJ)) + (1 << (LOGR + LOGJ - 4)) + 1);
+}
+
+// Butterfly b of a sub-stage with B = 2^lb butterflies per line -> (line, i).
+// Column mapping: lines fastest; row mapping: butterflies fastest.
+template <bool COLMAP, int LOGJ>
+NFFT_HD void lean_map(int b, int lb, int& l, int& i) {
+    if constexpr (COLMAP) { l = b & ((1 << LOGJ) - 1); i = b >> LOGJ; }
+    else { i = b & ((1 << lb) - 1); l = b >> lb; }
+}
+
+// x^0 .. x^15 by a depth-4 product tree.
+template <typename T>
+NFFT_HD void powers16(C2<T> x, C2<T>* p) {
+    p[0] = mkc((T)1, (T)0);
+    p[1] = x;
+    p[2] = cmul(x, x);
+    p[3] = cmul(p[2], x);
+    p[4] = cmul(p[2], p[2]);
+    p[8] = cmul(p[4], p[4]);
+    p[12] = cmul(p[8], p[4]);
+#pragma unroll
+    for (int a = 4; a < 16; a += 4) {
+        p[a + 1] = cmul(p[a], x);
+        p[a + 2] = cmul(p[a], p[2]);
+        p[a + 3] = cmul(p[a], p[3]);
+    }
+}
+
+// Per-line state held by every thread of the line.
+struct LeanLine {
+    long long bin, bout, j;
+};
+
+template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
+struct Lean {
+    static constexpr int THREADS = 1 << LOGT;
+    static constexpr int LOGTILE = LOGT + 4;
+    static constexpr int LOGJ = LOGTILE - LOGR;
+    static constexpr int J = 1 << LOGJ;
+    static constexpr int R = 1 << LOGR;
+    static constexpr bool PAIRED = (STORE == ST_R || STORE == ST_T2);
+    // shared layout: column tiles whenever either side walks lines
+    static constexpr bool COLL = COL_IN || COL_OUT;
+    static constexpr int NS = LeanSched<LOGR>::n;
+    static constexpr int SMEM_ELEMS = lean_smem_elems<COLL, LOGR, LOGJ>();
+    static_assert(LOGJ >= 0 && LOGJ <= 8, "tile must hold 1..256 lines");
+    static_assert(!(PAIRED && (COL_IN || COL_OUT)), "paired operators need whole contiguous lines");
+
+    // ---- first sub-stage: global -> registers -> radix 16 --------------------
+    static NFFT_HD void first(const PassArgs& a, const TwTables<T>* tw, const LeanLine* lines, int t, C2<T>* v, int& l,
+                              int& i) {
+        lean_map<COL_IN, LOGJ>(t, LOGR - 4, l, i);
+        const LeanLine ln = lines[l];
+        if (ln.j < 0) {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) v[m] = mkc((T)0, (T)0);
+            return;
+        }
+        if constexpr (LOAD == LD_C) {
+            const C2<T>* src = (const C2<T>*)a.in + ln.bin + ln.j * a.in_estride;
+            const long long rs = a.in_estride << a.logNj;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) v[m] = gload(&src[(long long)(i + (m << (LOGR - 4))) * rs], a.hint_in);
+            if (a.conj_in) {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < 16; ++m)
+                v[m] = load_elem<T, LOAD>(a, tw, ln.bin, ln.j + ((long long)(i + (m << (LOGR - 4))) << a.logNj));
+        }
+        if (a.logNs > 0) {
+            const long long k = ln.j & ((1ll << a.logNs) - 1);
+            if (k) {
+                // W_{Ns R}^{(i + m R/16) k} = W_{Ns R}^{i k} * (W_{16 Ns}^{k})^m
+                if (a.tw_mode == 2) {
+#pragma unroll
+                    for (int m = 0; m < 16; ++m)
+                        v[m] = cmul(v[m], twiddle<T>(tw, (uint64_t)(i + (m << (LOGR - 4))) * (uint64_t)k, a.logNs + LOGR));
+                } else if (a.tw_mode == 1) {
+                    C2<T> w = twiddle<T>(tw, (uint64_t)i * (uint64_t)k, a.logNs + LOGR);
+                    const C2<T> s = twiddle<T>(tw, (uint64_t)k, a.logNs + 4);
+                    const C2<T> s4 = cmul(cmul(s, s), cmul(s, s));
+                    // four interleaved chains w s^{4c + d}: depth 4 per chain
+                    C2<T> c0 = w, c1 = cmul(w, s);
+                    C2<T> c2 = cmul(c1, s), c3 = cmul(c2, s);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        v[4 * q + 0] = cmul(v[4 * q + 0], c0);
+                        v[4 * q + 1] = cmul(v[4 * q + 1], c1);
+                        v[4 * q + 2] = cmul(v[4 * q + 2], c2);
+                        v[4 * q + 3] = cmul(v[4 * q + 3], c3);
+                        if (q < 3) { c0 = cmul(c0, s4); c1 = cmul(c1, s4); c2 = cmul(c2, s4); c3 = cmul(c3, s4); }
+                    }
+                } else {
+                    C2<T> w0 = twiddle<T>(tw, (uint64_t)i * (uint64_t)k, a.logNs + LOGR);
+                    C2<T> s = twiddle<T>(tw, (uint64_t)k, a.logNs + 4);
+                    C2<T> p[16];
+                    powers16<T>(s, p);
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) v[m] = cmul(v[m], (m == 0) ? w0 : cmul(w0, p[m]));
+                }
+            }
+        }
+        dft16<T>(v);
+    }
+
+    // ---- middle / last sub-stage read from shared memory ----------------------
+    template <int S, bool COLMAP>
+    static NFFT_HD void read(const C2<T>* sm, int t, int q, C2<T>* v, int& l, int& i) {
+        constexpr int LR = LeanSched<LOGR>::lr[S];
+        constexpr int RHO = 1 << LR;
+        constexpr int lq = LOGR - LR;
+        lean_map<COLMAP, LOGJ>(t + q * THREADS, lq, l, i);
+#pragma unroll
+        for (int m = 0; m < RHO; ++m) v[m] = sm[NFFT_SM((lean_idx<COLL, LOGR, LOGJ>(l, i + (m << lq))))];
+    }
+
+    // internal twiddles W_{ns RHO}^{m k} and the radix-RHO DFT (ns = 2^lns)
+    template <int S>
+    static NFFT_HD void twiddle_dft(const TwTables<T>* tw, int i, C2<T>* v) {
+        constexpr int LR = LeanSched<LOGR>::lr[S];
+        constexpr int RHO = 1 << LR;
+        constexpr int lns = lns_of<S>();
+        const int k = i & ((1 << lns) - 1);
+        if (k) {
+#pragma unroll
+            for (int m = 1; m < RHO; ++m) {
+                C2<T> w = (lns + LR <= TW_BITS) ? twiddle_small<T>(tw, (uint32_t)(m * k), lns + LR)
+                                                : twiddle<T>(tw, (uint64_t)(m * k), lns + LR);
+                v[m] = cmul(v[m], w);
+            }
+        }
+        dft_radix<T, RHO>(v);
+    }
+
+    template <int S> static constexpr int lns_of() {
+        int s = 0;
+        for (int x = 0; x < S; ++x) s += LeanSched<LOGR>::lr[x];
+        return s;
+    }
+
+    // Stockham output position of sub-stage S (within the line)
+    template <int S>
+    static NFFT_HD int out_pos(int i, int m) {
+        constexpr int LR = LeanSched<LOGR>::lr[S];
+        constexpr int lns = lns_of<S>();
+        const int k = i & ((1 << lns) - 1);
+        return ((i >> lns) << (lns + LR)) + k + (m << lns);
+    }
+
+    template <int S>
+    static NFFT_HD void write_smem(C2<T>* sm, int l, int i, const C2<T>* v) {
+        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+#pragma unroll
+        for (int m = 0; m < RHO; ++m) sm[NFFT_SM((lean_idx<COLL, LOGR, LOGJ>(l, out_pos<S>(i, m))))] = v[m];
+    }
+
+    // last sub-stage: outputs straight to global memory
+    template <int S>
+    static NFFT_HD void write_global(const PassArgs& a, const TwTables<T>* tw, const LeanLine* lines, int l, int i,
+                                     const C2<T>* v) {
+        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+        const LeanLine ln = lines[l];
+        if (ln.j < 0) return;
+        const int logNso = a.logNs_out;
+        const long long base = ((ln.j >> logNso) << (logNso + LOGR)) + (ln.j & ((1ll << logNso) - 1));
+        if constexpr (STORE == ST_C) {
+            C2<T>* dst = (C2<T>*)a.out + ln.bout + base * a.out_estride;
+            const long long rs = a.out_estride << logNso;
+            const bool cj = a.conj_out, sc = a.scale != 1.0;
+            const T f = (T)a.scale;
+#pragma unroll
+            for (int m = 0; m < RHO; ++m) {
+                C2<T> x = v[m];
+                if (cj) x.y = -x.y;
+                if (sc) x = cscale(x, f);
+                gstore(&dst[(long long)out_pos<S>(i, m) * rs], x, a.hint_out);
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < RHO; ++m)
+                store_elem<T, STORE>(a, tw, ln.bout, base + ((long long)out_pos<S>(i, m) << logNso), v[m]);
+        }
+    }
+};
+
+template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
+constexpr size_t lean_smem_bytes() {
+    using L = Lean<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>;
+    return sizeof(C2<T>) * (size_t)L::SMEM_ELEMS + sizeof(LeanLine) * (size_t)L::J;
+}
+
+template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
+__global__ void __launch_bounds__(1 << LOGT, (LOGT <= 7 ? 4 : (LOGT == 8 ? 2 : 1)))
+lean_pass_kernel(const PassArgs a) {
+    using L = Lean<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>;
+    using V = C2<T>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    V* sm = (V*)smraw;
+    LeanLine* lines = (LeanLine*)(sm + L::SMEM_ELEMS);
+    const TwTables<T>* tw = (const TwTables<T>*)a.tw;
+    const int t = threadIdx.x;
+    const long long tile = (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x;
+    const long long line0 = tile << L::LOGJ;
+    if (line0 >= a.nlines) return;
+    if (t < L::J) {
+        long long tmp[3];
+        TileLines tl{&tmp[0], &tmp[1], &tmp[2]};
+        line_setup(a, line0 + t, 0, tl);
+        lines[t] = LeanLine{tmp[0], tmp[1], tmp[2]};
+    }
+    __syncthreads();
+
+    V v[16];
+    int l, i;
+    L::first(a, tw, lines, t, v, l, i);
+    if constexpr (L::NS == 1) {
+        // single radix-16 sub-stage: the same thread stores its outputs
+        if constexpr (L::PAIRED) {
+            L::template write_smem<0>(sm, l, i, v);
+        } else {
+            L::template write_global<0>(a, tw, lines, l, i, v);
+        }
+    } else {
+        L::template write_smem<0>(sm, l, i, v);
+        __syncthreads();
+        if constexpr (LOAD == LD_C && COL_IN) {
+            // every load of the tile has completed: drop the scratch lines just read
+            constexpr int PER_LINE = 128 / (int)sizeof(V);
+            if (a.discard_in && L::J >= PER_LINE && (l % PER_LINE) == 0) {
+                const LeanLine ln = lines[l];
+                if (ln.j >= 0) {
+                    const V* src = (const V*)a.in + ln.bin + ln.j * a.in_estride;
+                    const long long rs = a.in_estride << a.logNj;
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) discard_l2(&src[(long long)(i + (m << (LOGR - 4))) * rs]);
+                }
+            }
+        }
+        // middle sub-stages (compile-time unrolled)
+        if constexpr (L::NS >= 3) {
+            constexpr int S = 1;
+            constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+            V w[16];
+            int ls[16 / RHO], is[16 / RHO];
+#pragma unroll
+            for (int q = 0; q < 16 / RHO; ++q) L::template read<S, L::COLL>(sm, t, q, &w[q * RHO], ls[q], is[q]);
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 16 / RHO; ++q) {
+                L::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
+                L::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
+            }
+            __syncthreads();
+        }
+        if constexpr (L::NS >= 4) {
+            constexpr int S = 2;
+            constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+            V w[16];
+            int ls[16 / RHO], is[16 / RHO];
+#pragma unroll
+            for (int q = 0; q < 16 / RHO; ++q) L::template read<S, L::COLL>(sm, t, q, &w[q * RHO], ls[q], is[q]);
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 16 / RHO; ++q) {
+                L::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
+                L::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
+            }
+            __syncthreads();
+        }
+        // last sub-stage
+        {
+            constexpr int S = L::NS - 1;
+            constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+            V w[16];
+            int ls[16 / RHO], is[16 / RHO];
+#pragma unroll
+            for (int q = 0; q < 16 / RHO; ++q) L::template read<S, COL_OUT>(sm, t, q, &w[q * RHO], ls[q], is[q]);
+            if constexpr (L::PAIRED) __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 16 / RHO; ++q) {
+                L::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
+                if constexpr (L::PAIRED) L::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
+                else L::template write_global<S>(a, tw, lines, ls[q], is[q], &w[q * RHO]);
+            }
+        }
+    }
+    if constexpr (L::PAIRED) {
+        __syncthreads();
+        // whole lines in row layout: realdft unpack / DCT-2 post pairs
+        constexpr int ITEMS = (LOGR == 0) ? L::J : (L::J << (LOGR - 1));
+        for (int w = t; w < ITEMS; w += L::THREADS) {
+            int ll = w >> (LOGR - 1), k = w & ((1 << (LOGR - 1)) - 1);
+            const LeanLine ln = lines[ll];
+            if (ln.j < 0) continue;
+            unpack_pair<T, STORE>(a, tw, ln.bout, k, (long long)(1 << LOGR),
+                                  [&](long long r) { return sm[NFFT_SM((lean_idx<false, LOGR, L::LOGJ>(ll, (int)r)))]; });
+        }
+    }
+}
+
+}  // namespace nfft

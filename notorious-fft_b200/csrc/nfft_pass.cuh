@@ -75,6 +75,9 @@ struct PassArgs {
     int mid;                 // Bluestein middle pass: x filter, conj, second FFT
     int logM;                // log2 of the axis length for the fused middle pass
     int vjp;                 // adjoint weights (see the operators below)
+    int hint_in, hint_out;   // L2 policy of the complex input / output (gload / gstore)
+    int discard_in;          // input is scratch read for the last time: drop its L2 lines
+    int tw_mode;             // pass pre-twiddles: 0 product tree, 1 chained products, 2 table lookups
 };
 
 // Shared-memory index with one padding element every 16 (breaks the
@@ -318,22 +321,31 @@ NFFT_HD void line_setup(const PassArgs& a, long long lam, int l, TileLines tl) {
     tl.j[l] = j;
 }
 
-// Load tile slot e (0 <= e < J R) from global memory into shared memory.
+// Load of tile slot e (0 <= e < J R): the fused input operator's value.  The
+// kernel issues the loads of all its slots before consuming any of them.
 template <typename T, int LOAD>
-NFFT_HD void load_slot(const PassArgs& a, const TwTables<T>* tw, C2<T>* sm, TileLines tl, int e) {
+NFFT_HD C2<T> load_slot_value(const PassArgs& a, const TwTables<T>* tw, TileLines tl, int e) {
     const int logR = a.logR, logJ = a.logJ;
     int l, r;
     if (a.in_row) { l = e >> logR; r = e & ((1 << logR) - 1); }
     else { l = e & ((1 << logJ) - 1); r = e >> logJ; }
     long long j = tl.j[l];
-    C2<T> v = mkc((T)0, (T)0);
-    if (j >= 0) {
-        long long p = j + ((long long)r << a.logNj);
-        v = load_elem<T, LOAD>(a, tw, tl.in[l], p);
-        if (a.logNs > 0) {
-            long long k = j & ((1ll << a.logNs) - 1);
-            if (k) v = cmul(v, twiddle<T>(tw, (uint64_t)r * (uint64_t)k, a.logNs + logR));
-        }
+    if (j < 0) return mkc((T)0, (T)0);
+    long long p = j + ((long long)r << a.logNj);
+    return load_elem<T, LOAD>(a, tw, tl.in[l], p);
+}
+
+// Pass pre-twiddle W_{Ns R}^{r k} of slot e and its store into shared memory.
+template <typename T>
+NFFT_HD void load_slot_commit(const PassArgs& a, const TwTables<T>* tw, C2<T>* sm, TileLines tl, int e, C2<T> v) {
+    const int logR = a.logR, logJ = a.logJ;
+    int l, r;
+    if (a.in_row) { l = e >> logR; r = e & ((1 << logR) - 1); }
+    else { l = e & ((1 << logJ) - 1); r = e >> logJ; }
+    if (a.logNs > 0) {
+        long long j = tl.j[l];
+        long long k = j & ((1ll << a.logNs) - 1);
+        if (j >= 0 && k) v = cmul(v, twiddle<T>(tw, (uint64_t)r * (uint64_t)k, a.logNs + logR));
     }
     sm[NFFT_SM(spad((l << logR) + r))] = v;
 }
@@ -482,11 +494,19 @@ pass_kernel(const PassArgs a) {
 
     for (int l = tid; l < J; l += THREADS) line_setup(a, line0 + l, l, tl);
     __syncthreads();
-#pragma unroll 4
-    for (int it = 0; it < 16; ++it) {
-        int e = tid + it * THREADS;
-        if (e >= E) break;
-        load_slot<T, LOAD>(a, tw, sm, tl, e);
+    {
+        // all global loads of the slot set in flight before any is consumed
+        V buf[16];
+#pragma unroll
+        for (int it = 0; it < 16; ++it) {
+            int e = tid + it * THREADS;
+            if (e < E) buf[it] = load_slot_value<T, LOAD>(a, tw, tl, e);
+        }
+#pragma unroll
+        for (int it = 0; it < 16; ++it) {
+            int e = tid + it * THREADS;
+            if (e < E) load_slot_commit<T>(a, tw, sm, tl, e, buf[it]);
+        }
     }
     __syncthreads();
     tile_fft<T, THREADS>(sm, tw, a, logE, tid);
@@ -503,11 +523,10 @@ pass_kernel(const PassArgs a) {
         const int items = paired_items(a);
         for (int w = tid; w < items; w += THREADS) paired_slot<T, STORE>(a, tw, sm, tl, w);
     } else {
-#pragma unroll 4
+#pragma unroll
         for (int it = 0; it < 16; ++it) {
             int e = tid + it * THREADS;
-            if (e >= E) break;
-            store_slot<T, STORE>(a, tw, sm, tl, e);
+            if (e < E) store_slot<T, STORE>(a, tw, sm, tl, e);
         }
     }
 }

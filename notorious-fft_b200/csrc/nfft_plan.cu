@@ -178,6 +178,17 @@ static void* get_scratch(notorious_fft_plan* p, int slot, size_t bytes) {
     return ptr;
 }
 
+// NOTORIOUS_FFT_GENERIC_PASSES=1 routes every pass through pass_kernel (the
+// runtime-shaped kernel), e.g. to compare it with the specialized kernels.
+static bool lean_disabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NOTORIOUS_FFT_GENERIC_PASSES");
+        v = (e && atoi(e) != 0) ? 1 : 0;
+    }
+    return v == 1;
+}
+
 static size_t scratch_cap_bytes() {
     static size_t cap = 0;
     if (!cap) {
@@ -248,11 +259,45 @@ static void set_lines(PassArgs& a, const View& src, const View& dst, long long n
     a.nlines = n;
 }
 
+// L2 policy: NOTORIOUS_FFT_CACHE_HINTS=0 turns the hints off.
+static bool cache_hints() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NOTORIOUS_FFT_CACHE_HINTS");
+        v = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    return v == 1;
+}
+
+static int env_int(const char* name, int dflt) {
+    const char* e = getenv(name);
+    return e ? atoi(e) : dflt;
+}
+// Tuning knobs (defaults chosen from measurements on B200):
+//   NOTORIOUS_FFT_LEAN_LOGT  threads (log2) of the complex pass kernels
+//   NOTORIOUS_FFT_TW_MODE    pre-twiddle generation (0 tree, 1 chains, 2 tables)
+static int lean_logt_pref() {
+    static int v = env_int("NOTORIOUS_FFT_LEAN_LOGT", 8);
+    return v;
+}
+static int tw_mode() {
+    static int v = env_int("NOTORIOUS_FFT_TW_MODE", 1);
+    return v;
+}
+
+// in_scratch / out_scratch: the pass reads / writes an inter-pass scratch buffer.
 static bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR, int tile,
                      int nsub, const int* sub, const OpSpec& op, bool first, bool last, int mid, int logNs_out,
-                     const cplx_t* chirp, const cplx_t* filt, cudaStream_t s) {
+                     const cplx_t* chirp, const cplx_t* filt, cudaStream_t s, bool in_scratch = false,
+                     bool out_scratch = false) {
     PassArgs a;
     fill_common(a, c);
+    a.tw_mode = tw_mode();
+    if (cache_hints() && (in_scratch || out_scratch)) {
+        a.hint_in = in_scratch ? 2 : 1;
+        a.hint_out = out_scratch ? 2 : 1;
+        a.discard_in = in_scratch ? 1 : 0;
+    }
     a.in = src.ptr;
     a.out = dst.ptr;
     a.logR = logR;
@@ -290,6 +335,18 @@ static bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int l
     if (logJ < 0) {
         set_error(6, "pass radix 2^%d exceeds tile 2^%d", logR, tile);
         return false;
+    }
+    // specialized kernel for this pass shape when one is instantiated
+    if (!mid && logR >= 4 && !lean_disabled()) {
+        const int ci = a.in_row ? 0 : 1, co = a.out_row ? 0 : 1;
+        const bool rr = !ci && !co;
+        int logT = (logR <= 12 && (rr || logR <= 10)) ? 8 : 9;
+        if (lean_logt_pref() == 7 && lean_available(logR, 7, ci, co, ldop, stop)) logT = 7;
+        if (lean_available(logR, logT, ci, co, ldop, stop)) {
+            a.logJ = logT + 4 - logR;
+            long long nt = (a.nlines + (1ll << a.logJ) - 1) >> a.logJ;
+            return launch_lean(a, logT, ci, co, ldop, stop, nt, s);
+        }
     }
     a.logJ = logJ;
     long long ntiles = (a.nlines + (1ll << logJ) - 1) >> logJ;
@@ -378,7 +435,7 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
             }
             int logR = sch.plog[i];
             if (!run_pass(c, cur, out, logL, logNs, logR, sch.tile[i], sch.nsub[i], sch.sub[i], o, first, last, 0, logNs,
-                          nullptr, nullptr, s))
+                          nullptr, nullptr, s, /*in_scratch=*/!first, /*out_scratch=*/!to_user))
                 return false;
             logNs += logR;
             cur = out;

@@ -19,6 +19,7 @@
 #include <string.h>
 
 #include <map>
+#include <type_traits>
 #include <mutex>
 #include <vector>
 
@@ -139,6 +140,8 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 
 #include "../../notorious-fft_b200/csrc/nfft_plan.cu"
 #include "../../notorious-fft_b200/csrc/nfft_api.cu"
+#include "../../notorious-fft_b200/csrc/nfft_lean.cuh"
+#include "../../notorious-fft_b200/csrc/nfft_lean_list.h"
 
 // ---------------------------------------------------------------------------
 // emulated launches: the kernels' phase functions for every thread
@@ -195,7 +198,7 @@ static void emu_pass(const PassArgs& a, long long ntiles) {
             for (int it = 0; it < 16; ++it) {
                 int e = t + it * THREADS;
                 if (e >= E) break;
-                load_slot<T, LOAD>(a, tw, sm.data(), tl, e);
+                load_slot_commit<T>(a, tw, sm.data(), tl, e, load_slot_value<T, LOAD>(a, tw, tl, e));
             }
         fft();
         if (a.mid) {
@@ -294,6 +297,110 @@ bool launch_chirp(cplx_t* chirp, cplx_t* bwrap, long long n, long long M, cudaSt
 }
 
 bool set_kernel_attributes() { return true; }
+
+// ---- specialized (lean) pass kernels: the kernel body of nfft_lean.cuh, with
+// every phase run for all threads before the next (its __syncthreads points)
+template <int LOGR, int LOGT, bool CI, bool CO, int LD, int ST>
+static void emu_lean(const PassArgs& a, long long ntiles) {
+    using T = real_t;
+    using V = C2<T>;
+    using Lt = Lean<T, LOGR, LOGT, CI, CO, LD, ST>;
+    const TwTables<T>* tw = (const TwTables<T>*)a.tw;
+    constexpr int TH = Lt::THREADS;
+    g_smem_elems = Lt::SMEM_ELEMS;
+    std::vector<V> sm(Lt::SMEM_ELEMS);
+    std::vector<LeanLine> lines(Lt::J);
+    std::vector<V> regs((size_t)TH * 16);
+    std::vector<int> ls((size_t)TH * 16), is((size_t)TH * 16);
+    auto middle = [&](auto Sc) {
+        constexpr int S = decltype(Sc)::value;
+        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+        for (int t = 0; t < TH; ++t)
+            for (int q = 0; q < 16 / RHO; ++q)
+                Lt::template read<S, Lt::COLL>(sm.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
+        for (int t = 0; t < TH; ++t)
+            for (int q = 0; q < 16 / RHO; ++q) {
+                Lt::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
+                Lt::template write_smem<S>(sm.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
+            }
+    };
+    for (long long tile = 0; tile < ntiles; ++tile) {
+        const long long line0 = tile << Lt::LOGJ;
+        if (line0 >= a.nlines) continue;
+        for (auto& x : sm) x = mkc((T)NAN, (T)NAN);
+        for (int t = 0; t < Lt::J; ++t) {
+            long long tmp[3];
+            TileLines tl{&tmp[0], &tmp[1], &tmp[2]};
+            line_setup(a, line0 + t, 0, tl);
+            lines[t] = LeanLine{tmp[0], tmp[1], tmp[2]};
+        }
+        for (int t = 0; t < TH; ++t) {
+            int l, i;
+            Lt::first(a, tw, lines.data(), t, &regs[t * 16], l, i);
+            if constexpr (Lt::NS == 1) {
+                if constexpr (Lt::PAIRED) Lt::template write_smem<0>(sm.data(), l, i, &regs[t * 16]);
+                else Lt::template write_global<0>(a, tw, lines.data(), l, i, &regs[t * 16]);
+            } else {
+                Lt::template write_smem<0>(sm.data(), l, i, &regs[t * 16]);
+            }
+        }
+        if constexpr (Lt::NS >= 2) {
+            if constexpr (Lt::NS >= 3) middle(std::integral_constant<int, 1>{});
+            if constexpr (Lt::NS >= 4) middle(std::integral_constant<int, 2>{});
+            constexpr int S = Lt::NS - 1;
+            constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+            for (int t = 0; t < TH; ++t)
+                for (int q = 0; q < 16 / RHO; ++q)
+                    Lt::template read<S, CO>(sm.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
+            for (int t = 0; t < TH; ++t)
+                for (int q = 0; q < 16 / RHO; ++q) {
+                    Lt::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
+                    if constexpr (Lt::PAIRED)
+                        Lt::template write_smem<S>(sm.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
+                    else
+                        Lt::template write_global<S>(a, tw, lines.data(), ls[t * 16 + q], is[t * 16 + q],
+                                                     &regs[t * 16 + q * RHO]);
+                }
+        }
+        if constexpr (Lt::PAIRED) {
+            constexpr int ITEMS = Lt::J << (LOGR - 1);
+            for (int w = 0; w < ITEMS; ++w) {
+                int ll = w >> (LOGR - 1), k = w & ((1 << (LOGR - 1)) - 1);
+                const LeanLine ln = lines[ll];
+                if (ln.j < 0) continue;
+                unpack_pair<T, ST>(a, tw, ln.bout, k, (long long)(1 << LOGR),
+                                   [&](long long r) { return sm[NFFT_SM((lean_idx<false, LOGR, Lt::LOGJ>(ll, (int)r)))]; });
+            }
+        }
+    }
+}
+
+using EmuLean = void (*)(const PassArgs&, long long);
+static std::map<unsigned, EmuLean>& emu_lean_table() {
+    static std::map<unsigned, EmuLean> t = [] {
+        std::map<unsigned, EmuLean> m;
+#define X(R, T, CI, CO, LD, ST) m[lean_key(R, T, CI, CO, LD, ST)] = emu_lean<R, T, CI != 0, CO != 0, LD, ST>;
+        NFFT_LEAN_ALL(X)
+#undef X
+        return m;
+    }();
+    return t;
+}
+bool lean_available(int logR, int logT, int ci, int co, int ld, int st) {
+    return emu_lean_table().count(lean_key(logR, logT, ci, co, ld, st)) > 0;
+}
+static long long g_lean_launches = 0;
+bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, long long ntiles, cudaStream_t) {
+    auto it = emu_lean_table().find(lean_key(a.logR, logT, ci, co, ld, st));
+    if (it == emu_lean_table().end()) {
+        set_error(6, "no specialized pass kernel for radix 2^%d", a.logR);
+        return false;
+    }
+    g_launches++;
+    g_lean_launches++;
+    it->second(a, ntiles);
+    return true;
+}
 long long launch_count() { return g_launches; }
 
 }  // namespace nfft
@@ -314,5 +421,6 @@ void nfft_emu_unregister_host(void* p) {
     emu::host_ok.erase((uintptr_t)p);
 }
 long long nfft_emu_launches(void) { return nfft::g_launches; }
+long long nfft_emu_lean_launches(void) { return nfft::g_lean_launches; }
 long long nfft_emu_checks(void) { return emu::n_checks; }
 }

@@ -1,0 +1,234 @@
+"""Host logic on the CPU: the library's planner and C ABI compiled against an
+emulated CUDA runtime (tests/emu), running the kernels' own per-thread phase
+functions with every global and shared-memory access bounds-checked.
+
+Checks every transform family at single-pass, multi-pass and Bluestein
+sizes, N-D shapes (including the reference's length-1-axis rules), batched
+calls with padded distances, in-place calls, the error conventions of the C
+API, and the adjoints against the transposed transforms and finite
+differences.  Tolerances are the north-star ones (1e-13 log2 N for double,
+1e-6 log2 N for float).
+"""
+import math
+
+import numpy as np
+import pytest
+import scipy.fft as sf
+
+from oracle import rel_l2
+
+R2R = ["dct2", "dst2", "dct3", "dst3", "dct4", "dst4"]
+
+
+def tol(n, single=False):
+    return (1e-6 if single else 1e-13) * max(1.0, math.log2(max(n, 2)))
+
+
+def cx(rng, *shape):
+    return rng.uniform(-1, 1, shape) + 1j * rng.uniform(-1, 1, shape)
+
+
+@pytest.mark.parametrize("n", [1, 2, 4, 8, 16, 32, 64, 128, 512, 2048, 4096, 8192, 16384, 1 << 16])
+def test_emu_complex_pow2(emu_d, oracle_d, n):
+    x = cx(np.random.default_rng(n), n)
+    with emu_d.mkaux("dft", [n]) as a:
+        for k in ("dft", "invdft"):
+            assert rel_l2(a(k, x), oracle_d.transform(k, x)) <= tol(n), k
+
+
+@pytest.mark.parametrize("n", [3, 5, 6, 7, 10, 12, 15, 20, 100, 1000, 4097])
+def test_emu_bluestein(emu_d, oracle_d, n):
+    x = cx(np.random.default_rng(n), n)
+    with emu_d.mkaux("dft", [n]) as a:
+        for k in ("dft", "invdft"):
+            assert rel_l2(a(k, x), oracle_d.transform(k, x)) <= tol(n), k
+
+
+@pytest.mark.parametrize("n", [1, 2, 4, 8, 16, 64, 1024, 8192, 16384, 1 << 15, 1 << 16])
+def test_emu_real_families(emu_d, oracle_d, n):
+    rng = np.random.default_rng(n + 1)
+    x = rng.uniform(-1, 1, n)
+    with emu_d.mkaux("realdft", [n]) as a:
+        z = oracle_d.transform("realdft", x)
+        assert rel_l2(a("realdft", x), z) <= tol(n)
+        z2 = z + 0.25j * rng.uniform(-1, 1, z.shape)     # invrealdft ignores Im z_0, Im z_{N/2}
+        assert rel_l2(a("invrealdft", z2), oracle_d.invrealdft(z2, n)) <= tol(n)
+    with emu_d.mkaux("t2t3", [n]) as a:
+        for k in R2R[:4]:
+            assert rel_l2(a(k, x), oracle_d.transform(k, x)) <= tol(n), k
+    with emu_d.mkaux("t4", [n]) as a:
+        for k in R2R[4:]:
+            assert rel_l2(a(k, x), oracle_d.transform(k, x)) <= tol(n), k
+
+
+ND_SHAPES = [(4, 4), (8, 16), (32, 32), (4, 4, 4), (4, 8, 8), (1, 8), (8, 1), (1, 1), (2, 1, 4), (16, 1, 1),
+             (64, 128), (2048, 4), (2, 4096)]
+
+
+@pytest.mark.parametrize("dims", ND_SHAPES + [(3, 5), (6, 10, 12), (4, 3000)])
+def test_emu_nd_complex(emu_d, oracle_d, dims):
+    x = cx(np.random.default_rng(len(dims)), *dims)
+    with emu_d.mkaux("dft", dims) as a:
+        for k in ("dft", "invdft"):
+            assert rel_l2(a(k, x), oracle_d.nd(k, x)) <= tol(int(np.prod(dims))), k
+
+
+@pytest.mark.parametrize("dims", ND_SHAPES)
+def test_emu_nd_real(emu_d, oracle_d, dims):
+    rng = np.random.default_rng(7)
+    x = rng.uniform(-1, 1, dims)
+    n = int(np.prod(dims))
+    with emu_d.mkaux("t2t3", dims) as a:
+        for k in R2R[:4]:
+            assert rel_l2(a(k, x), oracle_d.nd(k, x)) <= tol(n), k
+    with emu_d.mkaux("t4", dims) as a:
+        for k in R2R[4:]:
+            assert rel_l2(a(k, x), oracle_d.nd(k, x)) <= tol(n), k
+    with emu_d.mkaux("realdft", dims) as a:
+        z = oracle_d.nd("realdft", x)
+        assert rel_l2(a("realdft", x), z) <= tol(n)
+        assert rel_l2(a("invrealdft", z), oracle_d.nd("invrealdft", z, dims)) <= tol(n)
+
+
+@pytest.mark.parametrize("n,B", [(64, 5), (4096, 3), (1 << 15, 2), (100, 4), (16384, 3)])
+def test_emu_batched_padded(emu_d, oracle_d, n, B):
+    rng = np.random.default_rng(n)
+    xb = cx(rng, B, n + 7)
+    yb = np.zeros((B, n + 3), complex)
+    with emu_d.mkaux("dft", [n]) as a:
+        a.batched("dft", xb, yb, B, n + 7, n + 3)
+    assert rel_l2(yb[:, :n], oracle_d.transform("dft", xb[:, :n])) <= tol(n)
+    if n & (n - 1) == 0:
+        xr = rng.uniform(-1, 1, (B, n + 5))
+        yr = np.zeros((B, n + 2))
+        with emu_d.mkaux("t2t3", [n]) as a:
+            a.batched("dct3", xr, yr, B, n + 5, n + 2)
+        assert rel_l2(yr[:, :n], oracle_d.transform("dct3", xr[:, :n])) <= tol(n)
+        zr = np.zeros((B, n // 2 + 3), complex)
+        with emu_d.mkaux("realdft", [n]) as a:
+            a.batched("realdft", xr, zr, B, n + 5, n // 2 + 3)
+        assert rel_l2(zr[:, :n // 2 + 1], oracle_d.transform("realdft", xr[:, :n])) <= tol(n)
+
+
+def test_emu_inplace(emu_d, oracle_d):
+    rng = np.random.default_rng(3)
+    for n in (1024, 1 << 15, 1000):
+        x = cx(rng, n)
+        y = x.copy()
+        with emu_d.mkaux("dft", [n]) as a:
+            emu_d._call(emu_d.lib.notorious_fft_dft, y, y, a)
+        assert rel_l2(y, oracle_d.transform("dft", x)) <= tol(n)
+
+
+def test_emu_float(emu_f, oracle_d):
+    rng = np.random.default_rng(11)
+    for n in (16, 4096, 1 << 15, 1000):
+        x = cx(rng, n).astype(np.complex64)
+        with emu_f.mkaux("dft", [n]) as a:
+            assert rel_l2(a("dft", x), oracle_d.transform("dft", x.astype(np.complex128))) <= tol(n, True)
+        if n & (n - 1) == 0:
+            xr = rng.uniform(-1, 1, n).astype(np.float32)
+            with emu_f.mkaux("t2t3", [n]) as a:
+                assert rel_l2(a("dct2", xr), oracle_d.transform("dct2", xr.astype(np.float64))) <= tol(n, True)
+
+
+# ---------------------------------------------------------------------------
+# C API conventions
+# ---------------------------------------------------------------------------
+def test_emu_null_conventions(emu_d):
+    for fam in ("realdft", "t2t3", "t4"):
+        assert not emu_d.mkaux_1d_raw(fam, 12)
+        assert not emu_d.mkaux_1d_raw(fam, 0)
+        assert emu_d.last_error()[0] == 1
+    assert not emu_d.mkaux_1d_raw("dft", 0)
+    assert not emu_d.mkaux_1d_raw("dft", -3)
+    p = emu_d.mkaux_1d_raw("dft", 12)
+    assert p
+    emu_d.free_raw(p)
+    emu_d.free_raw(None)
+    assert not emu_d.mkaux_raw("t2t3", [4, 6])      # any non-power-of-two dimension
+
+
+def test_emu_wrong_family_and_null_aux(emu_d):
+    x = np.zeros(16)
+    y = np.zeros(16)
+    with emu_d.mkaux("dft", [16]) as a:
+        with pytest.raises(Exception):
+            emu_d._call(emu_d.lib.notorious_fft_dct2, x, y, a)
+    emu_d.lib.notorious_fft_dct2(x.ctypes.data, y.ctypes.data, None)   # NULL aux: silent no-op + error code
+    assert emu_d.last_error()[0] == 1
+
+
+# ---------------------------------------------------------------------------
+# adjoints
+# ---------------------------------------------------------------------------
+def _real_view(a):
+    return np.concatenate([a.real.ravel(), a.imag.ravel()]) if np.iscomplexobj(a) else a.ravel()
+
+
+@pytest.mark.parametrize("kind", ["dft", "invdft", "realdft", "invrealdft"] + R2R)
+@pytest.mark.parametrize("dims", [(16,), (1000,), (8, 4), (1 << 15,)])
+def test_emu_vjp_inner_product(emu_d, kind, dims):
+    """<g, A x> == <A^T g, x> for random x, g (real inner product on pairs)."""
+    fam = {"dft": "dft", "invdft": "dft", "realdft": "realdft", "invrealdft": "realdft"}.get(kind, "t4" if kind in ("dct4", "dst4") else "t2t3")
+    if fam != "dft" and any(d & (d - 1) for d in dims):
+        pytest.skip("power-of-two only")
+    rng = np.random.default_rng(1)
+    with emu_d.mkaux(fam, dims) as a:
+        ins, outs = a.in_shape(kind), a.out_shape(kind)
+        cin = kind in ("dft", "invdft", "invrealdft")
+        cout = kind in ("dft", "invdft", "realdft")
+        x = cx(rng, *ins) if cin else rng.uniform(-1, 1, ins)
+        if kind == "invrealdft":
+            x = np.fft.rfftn(rng.uniform(-1, 1, dims))     # Hermitian-consistent input (edge bins real)
+        g = cx(rng, *outs) if cout else rng.uniform(-1, 1, outs)
+        y = a(kind, x)
+        gx = a.vjp(kind, g)
+    lhs = np.dot(_real_view(g), _real_view(y))
+    rhs = np.dot(_real_view(gx), _real_view(x))
+    assert abs(lhs - rhs) <= 1e-12 * max(1.0, abs(lhs)) * math.log2(max(np.prod(dims), 2))
+
+
+@pytest.mark.parametrize("kind", ["dct2", "dst3", "realdft", "dft"])
+def test_emu_vjp_finite_differences(emu_d, kind):
+    fam = {"dft": "dft", "realdft": "realdft"}.get(kind, "t2t3")
+    n = 64
+    rng = np.random.default_rng(5)
+    with emu_d.mkaux(fam, [n]) as a:
+        x = cx(rng, n) if kind == "dft" else rng.uniform(-1, 1, n)
+        outs = a.out_shape(kind)
+        g = cx(rng, *outs) if kind in ("dft", "realdft") else rng.uniform(-1, 1, outs)
+        gx = a.vjp(kind, g)
+
+        def L(v):
+            return np.dot(_real_view(g), _real_view(a(kind, v)))
+
+        h = 1e-6
+        for idx in rng.choice(n, 8, replace=False):
+            e = np.zeros(n)
+            e[idx] = 1
+            if kind == "dft":
+                for part, unit in ((np.real, 1.0), (np.imag, 1j)):
+                    fd = (L(x + h * unit * e) - L(x - h * unit * e)) / (2 * h)
+                    assert abs(fd - part(gx[idx])) < 1e-6 * max(1, abs(fd))
+            else:
+                fd = (L(x + h * e) - L(x - h * e)) / (2 * h)
+                assert abs(fd - gx[idx]) < 1e-6 * max(1, abs(fd))
+
+
+def test_emu_vjp_matches_reference_transform_on_cotangent(emu_d, oracle_d):
+    """The adjoint of DCT-2 is DCT-3 of the cotangent with entry 0 doubled
+    (and the others as defined), evaluated by the oracle's transforms."""
+    n = 256
+    g = np.random.default_rng(9).uniform(-1, 1, n)
+    with emu_d.mkaux("t2t3", [n]) as a:
+        gx = a.vjp("dct2", g)
+    gg = g.copy()
+    gg[0] *= 2
+    assert rel_l2(gx, oracle_d.transform("dct3", gg)) <= tol(n)
+    with emu_d.mkaux("realdft", [n]) as a:
+        gz = np.random.default_rng(10).uniform(-1, 1, n // 2 + 1) + 0j
+        gx = a.vjp("realdft", gz)
+    w = gz.copy()
+    w[1:-1] *= 0.5
+    assert rel_l2(gx, oracle_d.invrealdft(w, n)) <= tol(n)
