@@ -193,7 +193,7 @@ static size_t scratch_cap_bytes() {
     static size_t cap = 0;
     if (!cap) {
         const char* e = getenv("NOTORIOUS_FFT_SCRATCH_MB");
-        long mb = e ? atol(e) : 64;
+        long mb = e ? atol(e) : 512;
         if (mb < 1) mb = 1;
         cap = (size_t)mb << 20;
     }
@@ -277,7 +277,7 @@ static int env_int(const char* name, int dflt) {
 //   NOTORIOUS_FFT_LEAN_LOGT  threads (log2) of the complex pass kernels
 //   NOTORIOUS_FFT_TW_MODE    pre-twiddle generation (0 tree, 1 chains, 2 tables)
 static int lean_logt_pref() {
-    static int v = env_int("NOTORIOUS_FFT_LEAN_LOGT", 8);
+    static int v = env_int("NOTORIOUS_FFT_LEAN_LOGT", 7);
     return v;
 }
 static int tw_mode() {
