@@ -206,6 +206,23 @@ enum { NOTORIOUS_FFT_FORM_PLAIN = 0, NOTORIOUS_FFT_FORM_SPLIT_TC = 1 };
 int notorious_fft_set_form(notorious_fft_aux* a, int form);
 int notorious_fft_get_form(const notorious_fft_aux* a);
 
+/* Allocation-free batched complex DFT (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc -- code running inside another
+ * framework's memory manager, which owns the device heap, and latency-critical
+ * code that cannot take cudaMalloc's implicit device synchronization.  It
+ * runs `howmany` contiguous power-of-two transforms of length N
+ * (1 <= N <= 2^20; other lengths return NOTORIOUS_FFT_ERR_INVALID) from
+ * device memory x to device memory y (x == y allowed) on `stream`
+ * (a cudaStream_t, NULL for the legacy stream), forward (inverse = 0) or
+ * unnormalized inverse (inverse = 1), and allocates nothing: its scratch is a
+ * fixed 16 MiB __device__ array (plus the twiddle tables) that every GPU
+ * loading the library holds until exit.  The first call on a device resolves
+ * those arrays' addresses and fills the tables, waiting for that kernel, so it
+ * should come before any stream capture.  All calls share the scratch array:
+ * calls that overlap on the GPU race.  Returns 0 or an error code. */
+int notorious_fft_dft_noalloc(const notorious_fft_cmpl* x, notorious_fft_cmpl* y, int N, int howmany, int inverse,
+                              void* stream);
+
 /* Library identification: precision of this build's notorious_fft_real
  * (8 or 4) and a short version string. */
 int notorious_fft_real_size(void);

@@ -135,6 +135,26 @@ size_t out_elem_bytes(int kind);
 int plan_execute(notorious_fft_plan* p, int kind, const void* in, void* out, long long howmany,
                  long long idist, long long odist, cudaStream_t stream, int vjp = 0);
 
+// Fused operators of one transform (first-pass load / last-pass store).
+struct OpSpec {
+    int ld = LD_C, st = ST_C;
+    int conj_in = 0, conj_out = 0;
+    double scale = 1.0;
+    long long N = 0;
+    int logN = 0;
+    int dst = 0;
+    bool paired = false;   // st is ST_R / ST_T2 (needs whole lines or the unpack epilogue)
+    int vjp = 0;           // adjoint weights of the real operators
+};
+
+// One Stockham pass of an axis of length 2^logL (nfft_plan.cu).
+bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR, int tile,
+              int nsub, const int* sub, const OpSpec& op, bool first, bool last, int mid, int logNs_out,
+              const cplx_t* chirp, const cplx_t* filt, cudaStream_t s, bool in_scratch = false,
+              bool out_scratch = false);
+// Inter-pass scratch layout with the lines of `like` and axis length L.
+View scratch_view(void* ptr, const View& like, long long L, bool strided);
+
 // Kernel launchers (nfft_kernels.cu)
 bool launch_pass(const PassArgs& a, int load_op, int store_op, int log_tile, long long ntiles, cudaStream_t s);
 bool launch_unpack(const PassArgs& a, int store_op, const cplx_t* Z, long long zdist, long long nlines, cudaStream_t s);

@@ -1,0 +1,141 @@
+// nfft_noalloc.cu -- an allocation-free batched complex DFT.
+//
+// Some callers cannot call cudaMalloc: code that runs inside another
+// framework's memory manager, which owns the device heap and does not allow
+// direct driver allocations, and latency-critical code for which the
+// implicit device synchronization of cudaMalloc / cudaFree is not
+// acceptable.  notorious_fft_dft_noalloc serves them: it runs the same
+// Stockham passes as the regular multi-pass complex DFT, but its inter-pass
+// scratch and its twiddle tables live in file-scope __device__ arrays of a
+// fixed size instead of memory the library allocates.  Every GPU that loads
+// this library holds those arrays (16 MiB of scratch plus the tables) until
+// the process exits.
+//
+// The arrays are shared by every call: a call leaves its intermediate data
+// in the scratch array, and two calls whose kernels overlap on the GPU (for
+// example on two streams, or from two host threads) race on it.  The scratch
+// is always written before it is read, so nothing needs clearing.
+//
+// In host code the arrays' names are host-side stand-ins, not device
+// addresses, so the first call on each device looks up their device
+// addresses with cudaGetSymbolAddress (with that device current), fills the
+// twiddle tables with a kernel and waits for it.  That first call per device
+// should therefore come before any stream capture.
+#include <algorithm>
+#include <mutex>
+
+#include "../../include/notorious_fft.h"
+#include "nfft_engine.h"
+
+namespace {
+
+using namespace nfft;
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)16 << 20;
+constexpr long long NOALLOC_SCRATCH_ELEMS = (long long)(NOALLOC_SCRATCH_BYTES / sizeof(cplx_t));
+constexpr int NOALLOC_MAX_LOGN = 20;
+
+__device__ __align__(256) cplx_t g_noalloc_scratch[NOALLOC_SCRATCH_ELEMS];
+__device__ __align__(256) TwTables<real_t> g_noalloc_tw;
+
+struct NoallocDevice {
+    bool ready = false;
+    cplx_t* scratch = nullptr;
+    TwTables<real_t>* tw = nullptr;
+};
+std::mutex g_noalloc_mu;
+NoallocDevice g_noalloc_dev[64];
+
+// One-time set-up of the calling thread's current device (see the file header).
+NoallocDevice* noalloc_device() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        set_error(NOTORIOUS_FFT_ERR_NO_DEVICE, "no CUDA device available");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoallocDevice& d = g_noalloc_dev[dev];
+    if (d.ready) return &d;
+    void* scratch = nullptr;
+    void* tw = nullptr;
+    if (!cuda_ok(cudaGetSymbolAddress(&scratch, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)")) return nullptr;
+    if (!cuda_ok(cudaGetSymbolAddress(&tw, g_noalloc_tw), "cudaGetSymbolAddress(twiddle tables)")) return nullptr;
+    if (!set_kernel_attributes()) return nullptr;
+    if (!launch_init_tables((TwTables<real_t>*)tw, 0)) return nullptr;
+    if (!cuda_ok(cudaStreamSynchronize(0), "twiddle table set-up")) return nullptr;
+    d.scratch = (cplx_t*)scratch;
+    d.tw = (TwTables<real_t>*)tw;
+    d.ready = true;
+    return &d;
+}
+
+}  // namespace
+
+extern "C" int notorious_fft_dft_noalloc(const notorious_fft_cmpl* x, notorious_fft_cmpl* y, int N, int howmany,
+                                         int inverse, void* stream) {
+    clear_error();
+    if (!x || !y) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "NULL data pointer");
+        return NOTORIOUS_FFT_ERR_INVALID;
+    }
+    if (N < 1 || (N & (N - 1)) != 0 || N > (1 << NOALLOC_MAX_LOGN)) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID,
+                  "notorious_fft_dft_noalloc: N=%d must be a power of two <= %d (scratch limit %zu bytes per GPU); "
+                  "use notorious_fft_dft_batched for other lengths",
+                  N, 1 << NOALLOC_MAX_LOGN, NOALLOC_SCRATCH_BYTES);
+        return NOTORIOUS_FFT_ERR_INVALID;
+    }
+    if (howmany < 0) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "negative batch count");
+        return NOTORIOUS_FFT_ERR_INVALID;
+    }
+    if (((uintptr_t)x | (uintptr_t)y) % sizeof(cplx_t)) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "device pointers must be aligned to notorious_fft_cmpl");
+        return NOTORIOUS_FFT_ERR_INVALID;
+    }
+    if (howmany == 0) return 0;
+    NoallocDevice* d = noalloc_device();
+    if (!d) return last_error();
+    DeviceCtx ctx;
+    ctx.tw = d->tw;
+    cudaStream_t s = (cudaStream_t)stream;
+    int logN = 0;
+    while ((1 << logN) < N) ++logN;
+    const FftSchedule sch = make_schedule(logN, false);
+    OpSpec op;
+    op.conj_in = op.conj_out = inverse ? 1 : 0;
+    const long long L = N;
+    // whole transforms per scratch fill
+    const long long chunk = sch.npass == 1 ? howmany : std::max<long long>(1, NOALLOC_SCRATCH_ELEMS / L);
+    if (sch.npass > 2) {
+        set_error(NOTORIOUS_FFT_ERR_UNSUPPORTED, "schedule needs more than one scratch buffer");
+        return NOTORIOUS_FFT_ERR_UNSUPPORTED;
+    }
+    for (long long b0 = 0; b0 < howmany; b0 += chunk) {
+        const long long cn = std::min(chunk, (long long)howmany - b0);
+        View vs, vd;
+        vs.ptr = (void*)((const cplx_t*)x + b0 * L);
+        vd.ptr = (void*)((cplx_t*)y + b0 * L);
+        vs.estride = vd.estride = 1;
+        if (cn > 1) {
+            vs.nb = vd.nb = 1;
+            vs.cnt[0] = vd.cnt[0] = cn;
+            vs.str[0] = vd.str[0] = L;
+        }
+        if (sch.npass == 1) {
+            if (!run_pass(&ctx, vs, vd, logN, 0, sch.plog[0], sch.tile[0], sch.nsub[0], sch.sub[0], op, true, true, 0, 0,
+                          nullptr, nullptr, s))
+                return last_error() ? last_error() : NOTORIOUS_FFT_ERR_CUDA;
+            continue;
+        }
+        View mid = scratch_view(d->scratch, vs, L, false);
+        if (!run_pass(&ctx, vs, mid, logN, 0, sch.plog[0], sch.tile[0], sch.nsub[0], sch.sub[0], op, true, false, 0, 0,
+                      nullptr, nullptr, s, false, true))
+            return last_error() ? last_error() : NOTORIOUS_FFT_ERR_CUDA;
+        if (!run_pass(&ctx, mid, vd, logN, sch.plog[0], sch.plog[1], sch.tile[1], sch.nsub[1], sch.sub[1], op, false,
+                      true, 0, sch.plog[0], nullptr, nullptr, s, true, false))
+            return last_error() ? last_error() : NOTORIOUS_FFT_ERR_CUDA;
+    }
+    return 0;
+}

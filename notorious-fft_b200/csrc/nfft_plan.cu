@@ -203,16 +203,7 @@ static size_t scratch_cap_bytes() {
 // ---------------------------------------------------------------------------
 // pass construction
 // ---------------------------------------------------------------------------
-struct OpSpec {
-    int ld = LD_C, st = ST_C;
-    int conj_in = 0, conj_out = 0;
-    double scale = 1.0;
-    long long N = 0;
-    int logN = 0;
-    int dst = 0;
-    bool paired = false;   // st is ST_R / ST_T2 (needs whole lines or the unpack epilogue)
-    int vjp = 0;           // adjoint weights of the real operators
-};
+
 
 static void fill_common(PassArgs& a, const DeviceCtx* c) {
     memset(&a, 0, sizeof a);
@@ -286,10 +277,9 @@ static int tw_mode() {
 }
 
 // in_scratch / out_scratch: the pass reads / writes an inter-pass scratch buffer.
-static bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR, int tile,
-                     int nsub, const int* sub, const OpSpec& op, bool first, bool last, int mid, int logNs_out,
-                     const cplx_t* chirp, const cplx_t* filt, cudaStream_t s, bool in_scratch = false,
-                     bool out_scratch = false) {
+bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR, int tile,
+              int nsub, const int* sub, const OpSpec& op, bool first, bool last, int mid, int logNs_out,
+              const cplx_t* chirp, const cplx_t* filt, cudaStream_t s, bool in_scratch, bool out_scratch) {
     PassArgs a;
     fill_common(a, c);
     a.tw_mode = tw_mode();
@@ -355,7 +345,7 @@ static bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int l
 
 // Scratch view with the same lines as `like` and a contiguous (or, for
 // strided lines, unit-stride-batch-innermost) layout of axis length L.
-static View scratch_view(void* ptr, const View& like, long long L, bool strided) {
+View scratch_view(void* ptr, const View& like, long long L, bool strided) {
     View v;
     v.ptr = ptr;
     v.nb = like.nb;
