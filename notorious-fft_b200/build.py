@@ -26,11 +26,11 @@ LIB = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu", "nfft_noalloc.cu"] + [f"nfft_lean_s{k}.cu" for k in range(8)]
+SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu", "nfft_noalloc.cu", "nfft_cluster.cu"] + [f"nfft_lean_s{k}.cu" for k in range(8)]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 PRECISIONS = {
     "d": ("libnotorious_fft.so", ["-DNFFT_REAL=double"]),
-    "f": ("libnotorious_fftf.so", ["-DNFFT_REAL=float", "-DNOTORIOUS_FFT_SINGLE"]),
+    "f": ("libnotorious_fftf.so", ["-DNFFT_REAL=float", "-DNFFT_REAL_IS_FLOAT=1", "-DNOTORIOUS_FFT_SINGLE"]),
 }
 
 

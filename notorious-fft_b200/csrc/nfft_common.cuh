@@ -66,7 +66,7 @@ NFFT_HD void gstore(double2* p, double2 v, int hint) {
     if (hint == 1) { __stcs(p, v); return; }
     if (hint == 2) {
         uint64_t pol;
-        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
         asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y), "l"(pol)
                      : "memory");
         return;
@@ -83,7 +83,7 @@ NFFT_HD void gstore(float2* p, float2 v, int hint) {
     if (hint == 1) { __stcs(p, v); return; }
     if (hint == 2) {
         uint64_t pol;
-        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
         asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol)
                      : "memory");
         return;

@@ -164,6 +164,13 @@ bool launch_init_tables(TwTables<real_t>* tw, cudaStream_t s);
 bool launch_chirp(cplx_t* chirp, cplx_t* bwrap, long long n, long long M, cudaStream_t s);
 bool set_kernel_attributes();
 long long launch_count();
+void note_launch();
+
+// Cluster-resident complex DFT (nfft_cluster.cu): one transform of 2^logN
+// points per thread-block cluster; a1 / a2 are its two Stockham passes.
+bool cluster_available(int logN);
+int cluster_logr1(int logN);
+bool launch_cluster(const PassArgs& a1, const PassArgs& a2, int logN, long long ntransforms, cudaStream_t s);
 
 // Specialized pass kernels (nfft_lean.cuh), registered by the slice files.
 constexpr int NFFT_LEAN_SLICES = 8;

@@ -10,6 +10,7 @@ namespace nfft {
 // Kernels launched by this library in this process (all devices).
 static std::atomic<long long> g_launches{0};
 long long launch_count() { return g_launches.load(); }
+void note_launch() { g_launches++; }
 
 using PassFn = void (*)(const PassArgs);
 

@@ -82,6 +82,7 @@ struct Lean {
     static constexpr int LOGJ = LOGTILE - LOGR;
     static constexpr int J = 1 << LOGJ;
     static constexpr int R = 1 << LOGR;
+    static constexpr int LOGR_ = LOGR;
     static constexpr bool PAIRED = (STORE == ST_R || STORE == ST_T2);
     // shared layout: column tiles whenever either side walks lines
     static constexpr bool COLL = COL_IN || COL_OUT;
@@ -101,10 +102,16 @@ struct Lean {
             return;
         }
         if constexpr (LOAD == LD_C) {
-            const C2<T>* src = (const C2<T>*)a.in + ln.bin + ln.j * a.in_estride;
             const long long rs = a.in_estride << a.logNj;
+            const C2<T>* src = (const C2<T>*)a.in + ln.bin + ln.j * a.in_estride + (long long)i * rs;
+            const long long s16 = rs << (LOGR - 4);
+            if (a.hint_in) {
 #pragma unroll
-            for (int m = 0; m < 16; ++m) v[m] = gload(&src[(long long)(i + (m << (LOGR - 4))) * rs], a.hint_in);
+                for (int m = 0; m < 16; ++m) v[m] = gload(src + m * s16, 1);
+            } else {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) v[m] = NFFT_GLD(src + m * s16);
+            }
             if (a.conj_in) {
 #pragma unroll
                 for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
@@ -169,11 +176,21 @@ struct Lean {
         constexpr int lns = lns_of<S>();
         const int k = i & ((1 << lns) - 1);
         if (k) {
+            // W^{m k} for m < RHO from the root W^k by a product tree (depth <= 4)
+            const C2<T> w1 = (lns + LR <= TW_BITS) ? twiddle_small<T>(tw, (uint32_t)k, lns + LR)
+                                                   : twiddle<T>(tw, (uint64_t)k, lns + LR);
+            if constexpr (RHO == 16) {
+                C2<T> p[16];
+                powers16<T>(w1, p);
 #pragma unroll
-            for (int m = 1; m < RHO; ++m) {
-                C2<T> w = (lns + LR <= TW_BITS) ? twiddle_small<T>(tw, (uint32_t)(m * k), lns + LR)
-                                                : twiddle<T>(tw, (uint64_t)(m * k), lns + LR);
-                v[m] = cmul(v[m], w);
+                for (int m = 1; m < 16; ++m) v[m] = cmul(v[m], p[m]);
+            } else {
+                C2<T> w = w1;
+#pragma unroll
+                for (int m = 1; m < RHO; ++m) {
+                    v[m] = cmul(v[m], w);
+                    if (m + 1 < RHO) w = cmul(w, w1);
+                }
             }
         }
         dft_radix<T, RHO>(v);
@@ -211,16 +228,32 @@ struct Lean {
         const int logNso = a.logNs_out;
         const long long base = ((ln.j >> logNso) << (logNso + LOGR)) + (ln.j & ((1ll << logNso) - 1));
         if constexpr (STORE == ST_C) {
-            C2<T>* dst = (C2<T>*)a.out + ln.bout + base * a.out_estride;
             const long long rs = a.out_estride << logNso;
-            const bool cj = a.conj_out, sc = a.scale != 1.0;
-            const T f = (T)a.scale;
+            C2<T>* dst = (C2<T>*)a.out + ln.bout + base * a.out_estride + (long long)out_pos<S>(i, 0) * rs;
+            constexpr int lns = lns_of<S>();
+            const long long sm_ = rs << lns;   // output positions step by 2^lns per m
+            C2<T> x[RHO];
+            if (a.scale != 1.0) {
+                const T f = (T)a.scale;
+                const T fi = a.conj_out ? -f : f;
 #pragma unroll
-            for (int m = 0; m < RHO; ++m) {
-                C2<T> x = v[m];
-                if (cj) x.y = -x.y;
-                if (sc) x = cscale(x, f);
-                gstore(&dst[(long long)out_pos<S>(i, m) * rs], x, a.hint_out);
+                for (int m = 0; m < RHO; ++m) x[m] = mkc(v[m].x * f, v[m].y * fi);
+            } else if (a.conj_out) {
+#pragma unroll
+                for (int m = 0; m < RHO; ++m) x[m] = mkc(v[m].x, -v[m].y);
+            } else {
+#pragma unroll
+                for (int m = 0; m < RHO; ++m) x[m] = v[m];
+            }
+            if (a.hint_out == 2) {
+#pragma unroll
+                for (int m = 0; m < RHO; ++m) gstore(dst + m * sm_, x[m], 2);
+            } else if (a.hint_out == 1) {
+#pragma unroll
+                for (int m = 0; m < RHO; ++m) gstore(dst + m * sm_, x[m], 1);
+            } else {
+#pragma unroll
+                for (int m = 0; m < RHO; ++m) NFFT_GST(dst + m * sm_, x[m]);
             }
         } else {
 #pragma unroll

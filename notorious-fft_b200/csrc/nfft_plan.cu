@@ -380,6 +380,32 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
     const FftSchedule& sch = strided ? ax.fft_strided : ax.fft_contig;
     const long long L = 1ll << logL;
     const int np = sch.npass;
+    // One transform per thread-block cluster: no inter-pass scratch at all.
+    if (np > 1 && !strided && op.ld == LD_C && op.st == ST_C && src.nb <= 1 && dst.nb <= 1 &&
+        cluster_available(logL)) {
+        const int lr1 = cluster_logr1(logL), lr2 = logL - lr1;
+        PassArgs a1, a2;
+        fill_common(a1, c);
+        fill_common(a2, c);
+        a1.in = src.ptr;
+        a1.logR = lr1;
+        a1.logNj = lr2;
+        a1.in_estride = 1;
+        a1.conj_in = op.conj_in;
+        a1.istr[0] = src.nb ? src.str[0] : 0;
+        a1.hint_in = cache_hints() ? 1 : 0;
+        a2.out = dst.ptr;
+        a2.logR = lr2;
+        a2.logNs = lr1;
+        a2.logNs_out = lr1;
+        a2.logNj = lr1;
+        a2.out_estride = 1;
+        a2.conj_out = op.conj_out;
+        a2.scale = op.scale;
+        a2.ostr[0] = dst.nb ? dst.str[0] : 0;
+        a2.hint_out = cache_hints() ? 1 : 0;
+        return launch_cluster(a1, a2, logL, src.nb ? src.cnt[0] : 1, s);
+    }
     if (np == 1 && !(op.paired && strided)) {
         return run_pass(c, src, dst, logL, 0, sch.plog[0], sch.tile[0], sch.nsub[0], sch.sub[0], op, true, true, 0, 0,
                         nullptr, nullptr, s);

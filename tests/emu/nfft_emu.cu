@@ -142,6 +142,7 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 #include "../../notorious-fft_b200/csrc/nfft_api.cu"
 #include "../../notorious-fft_b200/csrc/nfft_lean.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_lean_list.h"
+#include "../../notorious-fft_b200/csrc/nfft_cluster.cuh"
 
 // ---------------------------------------------------------------------------
 // emulated launches: the kernels' phase functions for every thread
@@ -375,6 +376,100 @@ static void emu_lean(const PassArgs& a, long long ntiles) {
     }
 }
 
+// Middle and last sub-stages of a lean pass (nfft_cluster.cuh lean_tail),
+// every phase for all threads.
+template <typename P, bool TO_GLOBAL>
+static void emu_lean_tail(const PassArgs& a, const TwTables<real_t>* tw, std::vector<C2<real_t>>& sm,
+                          const LeanLine* lines) {
+    using V = C2<real_t>;
+    constexpr int TH = P::THREADS;
+    std::vector<V> regs((size_t)TH * 16);
+    std::vector<int> ls((size_t)TH * 16), is((size_t)TH * 16);
+    auto stage = [&](auto Sc, auto last) {
+        constexpr int S = decltype(Sc)::value;
+        constexpr bool LAST = decltype(last)::value;
+        constexpr int RHO = 1 << LeanSched<P::LOGR_>::lr[S];
+        for (int t = 0; t < TH; ++t)
+            for (int q = 0; q < 16 / RHO; ++q) {
+                if constexpr (LAST) P::template read<S, true>(sm.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
+                else P::template read<S, P::COLL>(sm.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
+            }
+        for (int t = 0; t < TH; ++t)
+            for (int q = 0; q < 16 / RHO; ++q) {
+                P::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
+                if constexpr (LAST && TO_GLOBAL)
+                    P::template write_global<S>(a, tw, lines, ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
+                else
+                    P::template write_smem<S>(sm.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
+            }
+    };
+    if constexpr (P::NS >= 3) stage(std::integral_constant<int, 1>{}, std::false_type{});
+    if constexpr (P::NS >= 4) stage(std::integral_constant<int, 2>{}, std::false_type{});
+    stage(std::integral_constant<int, P::NS - 1>{}, std::true_type{});
+}
+
+template <int R1, int R2, int LC, int LT>
+static void emu_cluster(const PassArgs& a1, const PassArgs& a2, long long ntransforms) {
+    using T = real_t;
+    using V = C2<T>;
+    using K = ClusterFFT<T, R1, R2, LC, LT>;
+    const TwTables<T>* tw = (const TwTables<T>*)a1.tw;
+    constexpr int C = 1 << LC, TH = 1 << LT;
+    g_smem_elems = K::SMEM_ELEMS;
+    std::vector<std::vector<V>> sm(C, std::vector<V>(K::SMEM_ELEMS));
+    std::vector<std::vector<LeanLine>> lines(C, std::vector<LeanLine>(K::MAXJ));
+    std::vector<V> regs((size_t)C * TH * 16);
+    std::vector<int> ls((size_t)C * TH), is((size_t)C * TH);
+    for (long long b = 0; b < ntransforms; ++b) {
+        for (int c = 0; c < C; ++c) {
+            for (auto& x : sm[c]) x = mkc((T)NAN, (T)NAN);
+            for (int l = 0; l < (1 << K::LOGJA); ++l) K::lines1(a1, b, c, l, lines[c].data());
+            for (int t = 0; t < TH; ++t) {
+                int l, i;
+                K::P1::first(a1, tw, lines[c].data(), t, &regs[((size_t)c * TH + t) * 16], l, i);
+                K::P1::template write_smem<0>(sm[c].data(), l, i, &regs[((size_t)c * TH + t) * 16]);
+            }
+            emu_lean_tail<typename K::P1, false>(a1, tw, sm[c], lines[c].data());
+        }
+        // cluster barrier; gather from every CTA's shared memory
+        for (int c = 0; c < C; ++c)
+            for (int t = 0; t < TH; ++t)
+                K::gather(a2, tw, c, t, [&](int rank) { return (const V*)sm[rank].data(); },
+                          &regs[((size_t)c * TH + t) * 16], ls[c * TH + t], is[c * TH + t]);
+        // cluster barrier; pass 2 finishes in each CTA
+        for (int c = 0; c < C; ++c) {
+            for (auto& x : sm[c]) x = mkc((T)NAN, (T)NAN);
+            for (int l = 0; l < (1 << K::LOGJC); ++l) K::lines2(a2, b, c, l, lines[c].data());
+            for (int t = 0; t < TH; ++t)
+                K::P2::template write_smem<0>(sm[c].data(), ls[c * TH + t], is[c * TH + t], &regs[((size_t)c * TH + t) * 16]);
+            emu_lean_tail<typename K::P2, true>(a2, tw, sm[c], lines[c].data());
+        }
+    }
+}
+
+bool cluster_available(int logN) {
+    // opt-in: on B200 the two-pass kernels are faster for now
+    const char* v = getenv("NOTORIOUS_FFT_CLUSTER");
+    if (!v || !atoi(v)) return false;
+    if (sizeof(real_t) == 4) return logN >= 14 && logN <= 17;
+    return logN >= 14 && logN <= 16;
+}
+int cluster_logr1(int logN) { return logN == 17 ? 8 : (logN == 14 ? 7 : (logN == 15 ? 7 : 8)); }
+static long long g_cluster_launches = 0;
+bool launch_cluster(const PassArgs& a1, const PassArgs& a2, int logN, long long ntransforms, cudaStream_t) {
+    g_launches++;
+    g_cluster_launches++;
+    switch (logN) {
+    case 14: emu_cluster<7, 7, 3, 7>(a1, a2, ntransforms); return true;
+    case 15: emu_cluster<7, 8, 3, 8>(a1, a2, ntransforms); return true;
+    case 16: emu_cluster<8, 8, 4, 8>(a1, a2, ntransforms); return true;
+    case 17: emu_cluster<8, 9, 4, 9>(a1, a2, ntransforms); return true;
+    }
+    set_error(6, "no cluster kernel for N = 2^%d", logN);
+    return false;
+}
+void note_launch() { g_launches++; }
+
 using EmuLean = void (*)(const PassArgs&, long long);
 static std::map<unsigned, EmuLean>& emu_lean_table() {
     static std::map<unsigned, EmuLean> t = [] {
@@ -422,5 +517,6 @@ void nfft_emu_unregister_host(void* p) {
 }
 long long nfft_emu_launches(void) { return nfft::g_launches; }
 long long nfft_emu_lean_launches(void) { return nfft::g_lean_launches; }
+long long nfft_emu_cluster_launches(void) { return nfft::g_cluster_launches; }
 long long nfft_emu_checks(void) { return emu::n_checks; }
 }
