@@ -36,6 +36,11 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "HBM GB/s, % roofline: FP64 drop-in vs batched split-TC form at stated error"
 
+# DRAM bytes per transform (dram__bytes_read.sum + dram__bytes_write.sum over
+# both pass kernels) from an ncu capture of 256 transforms of the same shape;
+# scaled to the batch for roofline.traffic.
+MEASURED_TRAFFIC_PER_TRANSFORM = {("c2c", 65536): 3.64e6}
+
 WORKLOADS = {
     "c2c": dict(N=65536, batch=4096, l2="inputs 4 GiB per array > L2 (no flush)", flush=False),
     "c1": dict(N=4096, batch=256, l2="L2 flushed (256 MiB write) between steps", flush=True),
@@ -156,6 +161,69 @@ def run_reference_arm(args, wl):
     print(json.dumps(line))
 
 
+def bench_float_forms(args, wl, x64, stream, ms_fp64, rank, world, dist):
+    """Plain FP32 and split-tensor-core FP32 forms on the FP64 run's shape:
+    GB/s (8-byte complex), transforms/s relative to the FP64 drop-in, and the
+    worst per-transform relative L2 error against the FP64 results of the same
+    inputs (a sample of the batch)."""
+    import torch
+
+    from notorious_fft import FORM_SPLIT_TC, load
+
+    Lf = load(single=True)
+    Lf.set_stream(stream.cuda_stream)
+    Ld = load(single=False)
+    N, B = wl["N"], wl["batch"]
+    xf = x64.to(torch.complex64)
+    yf = torch.empty_like(xf)
+    zf = torch.empty_like(xf)
+    out = {}
+    # FP64 reference results for a sample of the same (rounded) inputs
+    ns = min(B, 16)
+    xs = xf[:ns].to(torch.complex128)
+    ys = torch.empty_like(xs)
+    with Ld.mkaux("dft", [N]) as a64:
+        a64.batched("dft", xs, ys, ns, N, N)
+    torch.cuda.synchronize()
+    for name, form in (("fp32_plain", 0), ("split_tc", FORM_SPLIT_TC)):
+        aux = Lf.mkaux("dft", [N])
+        aux.set_form(form)
+
+        def step():
+            aux.batched("dft", xf, yf, B, N, N)
+            aux.batched("invdft", yf, zf, B, N, N)
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        if dist:
+            tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        aux.batched("dft", xf[:ns], yf[:ns], ns, N, N)
+        torch.cuda.synchronize()
+        d = (yf[:ns].to(torch.complex128) - ys)
+        errs = torch.linalg.vector_norm(d, dim=1) / torch.linalg.vector_norm(ys, dim=1)
+        aux.free()
+        gbs = 2 * B * 2 * N * 8 * world / (ms * 1e-3) / 1e9
+        out[name] = {"value": round(gbs, 1), "unit": "GB/s", "ms_per_step": round(ms, 4),
+                     "transforms_per_s": round(2 * B * world / (ms * 1e-3), 1),
+                     "speedup_vs_fp64_transforms": round(ms_fp64 / ms, 3),
+                     "max_rel_l2_vs_fp64": float(errs.max().item()), "error_sample_transforms": ns,
+                     "dtype": "f32 storage" + (", radix-16 as fp16 hi+lo tensor-core products" if form else "")}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -166,6 +234,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="override the workload's batch (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the float-library forms")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.batch:
@@ -248,9 +317,17 @@ def main():
     # the batch), timed with CUDA events on the launching stream
     per_transform_ms = ms_step / 2
     achieved = (B * 2 * N * 16) / (per_transform_ms * 1e-3) / 1e9
+    tpt = MEASURED_TRAFFIC_PER_TRANSFORM.get((args.workload, N))
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
-            "kernel": "pass_kernel<double> x passes (one batched c2c transform)"}
+            "frac": round(achieved / peak, 4), "traffic": (round(tpt * B) if tpt else None),
+            "traffic_unit": "bytes per batched transform (ncu, scaled from 256 transforms)",
+            "algorithmic_bytes": B * 2 * N * 16, "peak_kind": peak_kind,
+            "kernel": "lean_pass_kernel<double> pass 1 + pass 2 (one batched c2c transform of N=65536)"}
+
+    # ---- the float library on the same shape: plain FP32 and split tensor-core form ----
+    forms = {}
+    if not args.no_forms:
+        forms = bench_float_forms(args, wl, x, stream, ms_step, rank, world, dist)
 
     e2e = None
     if not args.no_e2e and rank == 0 and world == 1:
@@ -288,6 +365,7 @@ def main():
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": ck, "round_trip_rel_err": err,
         }
+        line.update(forms)
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

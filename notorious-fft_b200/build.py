@@ -26,7 +26,7 @@ LIB = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu", "nfft_noalloc.cu", "nfft_cluster.cu"] + [f"nfft_lean_s{k}.cu" for k in range(8)]
+SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu", "nfft_noalloc.cu", "nfft_cluster.cu", "nfft_tc.cu"] + [f"nfft_lean_s{k}.cu" for k in range(8)]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 PRECISIONS = {
     "d": ("libnotorious_fft.so", ["-DNFFT_REAL=double"]),

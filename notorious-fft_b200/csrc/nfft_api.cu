@@ -6,6 +6,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+
 #include "../../include/notorious_fft.h"
 #include "nfft_engine.h"
 
@@ -32,6 +34,78 @@ notorious_fft_aux* make_aux(int family, int d, const int* Ns) {
     a->N = (int)total;
     a->plan = p;
     return a;
+}
+
+bool grow(void** buf, size_t* have, size_t need);
+
+bool is_pinned_host_ptr(const void* ptr) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeHost;
+}
+
+// Batched call with both buffers in pinned host memory: the batch goes through
+// the GPU in chunks, with the copy-in of chunk k+1 and the copy-out of chunk
+// k-1 overlapping the transform of chunk k (copy engines in both directions
+// plus the compute stream).  Transforms stay ordered on the caller's stream, so
+// the plan's scratch is never used by two chunks at once.
+bool run_pipelined(notorious_fft_plan* p, int kind, const void* x, void* y, long long howmany, long long idist,
+                   long long odist, long long in_elems, long long out_elems, size_t in_eb, size_t out_eb, int vjp,
+                   cudaStream_t s) {
+    const size_t target = (size_t)64 << 20;
+    long long chunk = (long long)(target / std::max<size_t>((size_t)idist * in_eb, 1));
+    if (chunk < 1) chunk = 1;
+    if (chunk > howmany) chunk = howmany;
+    const size_t cin = (size_t)((chunk - 1) * idist + in_elems) * in_eb;
+    const size_t cout = (size_t)((chunk - 1) * odist + out_elems) * out_eb;
+    if (!p->s_h2d) {
+        if (!cuda_ok(cudaStreamCreateWithFlags(&p->s_h2d, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+        if (!cuda_ok(cudaStreamCreateWithFlags(&p->s_d2h, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+        for (int i = 0; i < 2; ++i) {
+            if (!cuda_ok(cudaEventCreateWithFlags(&p->ev_h[i], cudaEventDisableTiming), "cudaEventCreate") ||
+                !cuda_ok(cudaEventCreateWithFlags(&p->ev_c[i], cudaEventDisableTiming), "cudaEventCreate") ||
+                !cuda_ok(cudaEventCreateWithFlags(&p->ev_d[i], cudaEventDisableTiming), "cudaEventCreate"))
+                return false;
+        }
+    }
+    if (!grow(&p->stage_in, &p->stage_in_bytes, 2 * cin)) return false;
+    if (!grow(&p->stage_out, &p->stage_out_bytes, 2 * cout)) return false;
+    char* in_st[2] = {(char*)p->stage_in, (char*)p->stage_in + cin};
+    char* out_st[2] = {(char*)p->stage_out, (char*)p->stage_out + cout};
+    // the staging buffers must not be rewritten while earlier work still reads them
+    cudaEvent_t start;
+    if (!cuda_ok(cudaEventCreateWithFlags(&start, cudaEventDisableTiming), "cudaEventCreate")) return false;
+    cudaEventRecord(start, s);
+    cudaStreamWaitEvent(p->s_h2d, start, 0);
+    cudaStreamWaitEvent(p->s_d2h, start, 0);
+    bool ok = true;
+    long long k = 0;
+    for (long long b0 = 0; b0 < howmany && ok; b0 += chunk, ++k) {
+        const long long cn = std::min(chunk, howmany - b0);
+        const int buf = (int)(k & 1);
+        const size_t nin = (size_t)((cn - 1) * idist + in_elems) * in_eb;
+        const size_t nout = (size_t)((cn - 1) * odist + out_elems) * out_eb;
+        if (k >= 2) cudaStreamWaitEvent(p->s_h2d, p->ev_c[buf], 0);
+        ok = cuda_ok(cudaMemcpyAsync(in_st[buf], (const char*)x + (size_t)b0 * idist * in_eb, nin,
+                                     cudaMemcpyHostToDevice, p->s_h2d), "H2D copy");
+        ok = ok && cuda_ok(cudaEventRecord(p->ev_h[buf], p->s_h2d), "cudaEventRecord");
+        ok = ok && cuda_ok(cudaStreamWaitEvent(s, p->ev_h[buf], 0), "cudaStreamWaitEvent");
+        if (ok && k >= 2) ok = cuda_ok(cudaStreamWaitEvent(s, p->ev_d[buf], 0), "cudaStreamWaitEvent");
+        ok = ok && plan_execute(p, kind, in_st[buf], out_st[buf], cn, idist, odist, s, vjp) == 0;
+        ok = ok && cuda_ok(cudaEventRecord(p->ev_c[buf], s), "cudaEventRecord");
+        ok = ok && cuda_ok(cudaStreamWaitEvent(p->s_d2h, p->ev_c[buf], 0), "cudaStreamWaitEvent");
+        ok = ok && cuda_ok(cudaMemcpyAsync((char*)y + (size_t)b0 * odist * out_eb, out_st[buf], nout,
+                                           cudaMemcpyDeviceToHost, p->s_d2h), "D2H copy");
+        ok = ok && cuda_ok(cudaEventRecord(p->ev_d[buf], p->s_d2h), "cudaEventRecord");
+    }
+    ok = cuda_ok(cudaStreamSynchronize(p->s_d2h), "stream synchronize") && ok;
+    ok = cuda_ok(cudaStreamSynchronize(s), "stream synchronize") && ok;
+    ok = cuda_ok(cudaStreamSynchronize(p->s_h2d), "stream synchronize") && ok;
+    cudaEventDestroy(start);
+    return ok;
 }
 
 bool is_device_ptr(const void* ptr) {
@@ -98,6 +172,10 @@ void run(int kind, const void* x, void* y, const notorious_fft_aux* a, long long
     cudaStream_t s = t_stream;
     const void* din = x;
     void* dout = y;
+    if (!xd && !yd && howmany >= 4 && (x != y || idist == odist) && is_pinned_host_ptr(x) && is_pinned_host_ptr(y)) {
+        run_pipelined(p, kind, x, y, howmany, idist, odist, in_elems, out_elems, in_eb, out_eb, vjp, s);
+        goto done;
+    }
     if (!xd) {
         if (!grow(&p->stage_in, &p->stage_in_bytes, in_bytes)) goto done;
         if (!cuda_ok(cudaMemcpyAsync(p->stage_in, x, in_bytes, cudaMemcpyHostToDevice, s), "H2D copy")) goto done;
@@ -267,8 +345,12 @@ int notorious_fft_set_form(notorious_fft_aux* a, int form) {
         return 0;
     }
     if (form == NOTORIOUS_FFT_FORM_SPLIT_TC) {
-        set_error(NOTORIOUS_FFT_ERR_UNSUPPORTED, "the split tensor-core form is not available in this build");
-        return NOTORIOUS_FFT_ERR_UNSUPPORTED;
+        if (sizeof(real_t) != 4) {
+            set_error(NOTORIOUS_FFT_ERR_UNSUPPORTED, "the split tensor-core form is a float-library form");
+            return NOTORIOUS_FFT_ERR_UNSUPPORTED;
+        }
+        a->plan->form = form;
+        return 0;
     }
     set_error(NOTORIOUS_FFT_ERR_INVALID, "unknown form %d", form);
     return NOTORIOUS_FFT_ERR_INVALID;

@@ -114,6 +114,9 @@ struct notorious_fft_plan {
     void* stage_in = nullptr;
     void* stage_out = nullptr;
     size_t stage_in_bytes = 0, stage_out_bytes = 0;
+    // pipelined host-pointer calls: copy streams, events, double-buffered staging
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+    cudaEvent_t ev_h[2] = {nullptr, nullptr}, ev_c[2] = {nullptr, nullptr}, ev_d[2] = {nullptr, nullptr};
     // temporary of the multi-dimensional inverse real transform
     void* nd_tmp = nullptr;
     size_t nd_tmp_bytes = 0;
@@ -145,6 +148,7 @@ struct OpSpec {
     int dst = 0;
     bool paired = false;   // st is ST_R / ST_T2 (needs whole lines or the unpack epilogue)
     int vjp = 0;           // adjoint weights of the real operators
+    int tc = 0;            // split tensor-core radix-16 sub-stages (float library)
 };
 
 // One Stockham pass of an axis of length 2^logL (nfft_plan.cu).
@@ -169,6 +173,8 @@ void note_launch();
 // Cluster-resident complex DFT (nfft_cluster.cu): one transform of 2^logN
 // points per thread-block cluster; a1 / a2 are its two Stockham passes.
 bool cluster_available(int logN);
+// Split-tensor-core pass (nfft_tc.cu, float library): LD_C / ST_C passes.
+bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStream_t s);
 int cluster_logr1(int logN);
 bool launch_cluster(const PassArgs& a1, const PassArgs& a2, int logN, long long ntransforms, cudaStream_t s);
 

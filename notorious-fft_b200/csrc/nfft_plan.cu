@@ -326,6 +326,12 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
         set_error(6, "pass radix 2^%d exceeds tile 2^%d", logR, tile);
         return false;
     }
+    // split tensor-core form: radix-16 sub-stages on the tensor cores
+    if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR >= 4 && tile == 12 && logJ == 12 - logR) {
+        a.logJ = logJ;
+        long long nt = (a.nlines + (1ll << logJ) - 1) >> logJ;
+        return launch_tc_pass(a, tile, nt, s);
+    }
     // specialized kernel for this pass shape when one is instantiated
     if (!mid && logR >= 4 && !lean_disabled()) {
         const int ci = a.in_row ? 0 : 1, co = a.out_row ? 0 : 1;
@@ -381,7 +387,7 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
     const long long L = 1ll << logL;
     const int np = sch.npass;
     // One transform per thread-block cluster: no inter-pass scratch at all.
-    if (np > 1 && !strided && op.ld == LD_C && op.st == ST_C && src.nb <= 1 && dst.nb <= 1 &&
+    if (np > 1 && !strided && !op.tc && op.ld == LD_C && op.st == ST_C && src.nb <= 1 && dst.nb <= 1 &&
         cluster_available(logL)) {
         const int lr1 = cluster_logr1(logL), lr2 = logL - lr1;
         PassArgs a1, a2;
@@ -657,6 +663,13 @@ void plan_destroy(notorious_fft_plan* p) {
     for (int i = 0; i < 2; ++i)
         if (p->scratch[i]) cudaFree(p->scratch[i]);
     if (p->stage_in) cudaFree(p->stage_in);
+    for (int i = 0; i < 2; ++i) {
+        if (p->ev_h[i]) cudaEventDestroy(p->ev_h[i]);
+        if (p->ev_c[i]) cudaEventDestroy(p->ev_c[i]);
+        if (p->ev_d[i]) cudaEventDestroy(p->ev_d[i]);
+    }
+    if (p->s_h2d) cudaStreamDestroy(p->s_h2d);
+    if (p->s_d2h) cudaStreamDestroy(p->s_d2h);
     if (p->nd_tmp) cudaFree(p->nd_tmp);
     if (p->stage_out) cudaFree(p->stage_out);
     if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
@@ -805,6 +818,7 @@ int plan_execute(notorious_fft_plan* p, int okind, const void* in, void* out, lo
             if (ax.pow2) {
                 OpSpec op;
                 op.conj_in = op.conj_out = inverse;
+                op.tc = p->form == 1 ? 1 : 0;
                 ok = run_pow2_axis(p, c, ax, src, dst, op, stream);
             } else {
                 ok = run_bluestein_axis(p, c, ax, src, dst, inverse, scale_blue ? 1.0 / (double)ax.n : 1.0, stream);

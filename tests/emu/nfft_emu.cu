@@ -100,7 +100,26 @@ cudaError_t GetDeviceProperties(cudaDeviceProp* p, int) {
 }
 cudaError_t PointerGetAttributes(cudaPointerAttributes* a, const void* p) {
     memset(a, 0, sizeof *a);
-    a->type = is_dev(p, 1) ? cudaMemoryTypeDevice : cudaMemoryTypeUnregistered;
+    bool pinned;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        pinned = inside(host_ok, (uintptr_t)p, 1);
+    }
+    // buffers registered by the tests stand for pinned host memory
+    a->type = is_dev(p, 1) ? cudaMemoryTypeDevice : (pinned ? cudaMemoryTypeHost : cudaMemoryTypeUnregistered);
+    return cudaSuccess;
+}
+// streams and events: the emulator runs everything synchronously
+cudaError_t StreamCreateWithFlags(cudaStream_t* s, unsigned) {
+    static int dummy[64];
+    static int n = 0;
+    *s = (cudaStream_t)&dummy[(n++) & 63];
+    return cudaSuccess;
+}
+cudaError_t EventCreateWithFlags(cudaEvent_t* e, unsigned) {
+    static int dummy[256];
+    static int n = 0;
+    *e = (cudaEvent_t)&dummy[(n++) & 255];
     return cudaSuccess;
 }
 const char* ErrorString(cudaError_t) { return "emulated CUDA error"; }
@@ -137,12 +156,19 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 #define cudaPointerGetAttributes emu::PointerGetAttributes
 #define cudaGetLastError() emu::Ok()
 #define cudaGetErrorString emu::ErrorString
+#define cudaStreamCreateWithFlags emu::StreamCreateWithFlags
+#define cudaEventCreateWithFlags emu::EventCreateWithFlags
+#define cudaEventRecord(e, s) emu::Ok()
+#define cudaStreamWaitEvent(s, e, f) emu::Ok()
+#define cudaEventDestroy(e) emu::Ok()
+#define cudaStreamDestroy(s) emu::Ok()
 
 #include "../../notorious-fft_b200/csrc/nfft_plan.cu"
 #include "../../notorious-fft_b200/csrc/nfft_api.cu"
 #include "../../notorious-fft_b200/csrc/nfft_lean.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_lean_list.h"
 #include "../../notorious-fft_b200/csrc/nfft_cluster.cuh"
+#include "../../notorious-fft_b200/csrc/nfft_tc.cuh"
 
 // ---------------------------------------------------------------------------
 // emulated launches: the kernels' phase functions for every thread
@@ -469,6 +495,158 @@ bool launch_cluster(const PassArgs& a1, const PassArgs& a2, int logN, long long 
     return false;
 }
 void note_launch() { g_launches++; }
+
+// ---- split tensor-core pass: a host model of mma.sync.m16n8k16 (f16 x f16
+// -> f32) from the fragment layout documented in nfft_tc.cuh, and the
+// tc_substage phases for every lane of every warp.
+static void emu_mma(const uint32_t (*a)[4], const uint32_t (*b)[2], float (*d)[4]) {
+    float A[16][16], B[16][8];
+    auto lo = [](uint32_t v) { return __half2float(__ushort_as_half((unsigned short)(v & 0xffff))); };
+    auto hi = [](uint32_t v) { return __half2float(__ushort_as_half((unsigned short)(v >> 16))); };
+    for (int lane = 0; lane < 32; ++lane) {
+        int g = lane >> 2, t4 = lane & 3;
+        for (int r = 0; r < 4; ++r) {
+            int row = g + 8 * (r & 1), col = 2 * t4 + 8 * (r >> 1);
+            A[row][col] = lo(a[lane][r]);
+            A[row][col + 1] = hi(a[lane][r]);
+        }
+        for (int r = 0; r < 2; ++r) {
+            int k = 2 * t4 + 8 * r;
+            B[k][g] = lo(b[lane][r]);
+            B[k + 1][g] = hi(b[lane][r]);
+        }
+    }
+    for (int lane = 0; lane < 32; ++lane) {
+        int g = lane >> 2, t4 = lane & 3;
+        for (int r = 0; r < 4; ++r) {
+            int row = g + 8 * (r >> 1), col = 2 * t4 + (r & 1);
+            float acc = d[lane][r];
+            for (int k = 0; k < 16; ++k) acc += A[row][k] * B[k][col];
+            d[lane][r] = acc;
+        }
+    }
+}
+
+template <int THREADS>
+static void emu_tc_substage(std::vector<C2<real_t>>& smv, const TwTables<real_t>* tw, int logR, int logE, int lns) {
+    if constexpr (sizeof(real_t) == 4) {
+        float2* sm = (float2*)smv.data();
+        const TwTables<float>* twf = (const TwTables<float>*)tw;
+        const int nbf = 1 << (logE - 4);
+        const int W = THREADS / 32;
+        std::vector<float2> x((size_t)W * 32 * 16);
+        std::vector<int> ls((size_t)W * 32 * 4), is((size_t)W * 32 * 4);
+        for (int w = 0; w < W; ++w)
+            for (int lane = 0; lane < 32; ++lane)
+                for (int q = 0; q < 4; ++q) {
+                    float2* xp = &x[(((size_t)w * 32 + lane) * 4 + q) * 4];
+                    int& l = ls[((size_t)w * 32 + lane) * 4 + q];
+                    int& i = is[((size_t)w * 32 + lane) * 4 + q];
+                    if (w * 32 + q * 8 + (lane >> 2) < nbf) tc_read(sm, logR, lns, w, q, lane, xp, l, i);
+                    else { for (int p = 0; p < 4; ++p) xp[p] = make_float2(0.f, 0.f); i = 0; }
+                }
+        TcA A[32];
+        for (int lane = 0; lane < 32; ++lane) tc_make_A(lane, A[lane]);
+        for (int w = 0; w < W; ++w)
+            for (int q = 0; q < 4; ++q) {
+                if (w * 32 + q * 8 >= nbf) continue;
+                float sc[32], amax[32];
+                for (int lane = 0; lane < 32; ++lane) {
+                    float2* xp = &x[(((size_t)w * 32 + lane) * 4 + q) * 4];
+                    tc_twiddle(twf, lns, is[((size_t)w * 32 + lane) * 4 + q], lane, xp);
+                    float m = 0.f;
+                    for (int p = 0; p < 4; ++p) m = fmaxf(m, fmaxf(fabsf(xp[p].x), fabsf(xp[p].y)));
+                    amax[lane] = m;
+                }
+                for (int lane = 0; lane < 32; ++lane) {
+                    int b0 = lane & ~3;
+                    float m = fmaxf(fmaxf(amax[b0], amax[b0 + 1]), fmaxf(amax[b0 + 2], amax[b0 + 3]));
+                    sc[lane] = tc_scale(m);
+                }
+                uint32_t a_rl[32][4], a_rh[32][4], a_il[32][4], a_ih[32][4], a_nil[32][4], a_nih[32][4];
+                uint32_t b_rh[32][2], b_rl[32][2], b_ih[32][2], b_il[32][2];
+                for (int lane = 0; lane < 32; ++lane) {
+                    float2* xp = &x[(((size_t)w * 32 + lane) * 4 + q) * 4];
+                    for (int p = 0; p < 4; ++p) xp[p] = make_float2(xp[p].x * sc[lane], xp[p].y * sc[lane]);
+                    TcB B;
+                    tc_make_B(xp, B);
+                    for (int r = 0; r < 4; ++r) {
+                        a_rl[lane][r] = A[lane].rl[r]; a_rh[lane][r] = A[lane].rh[r];
+                        a_il[lane][r] = A[lane].il[r]; a_ih[lane][r] = A[lane].ih[r];
+                        a_nil[lane][r] = A[lane].nil[r]; a_nih[lane][r] = A[lane].nih[r];
+                    }
+                    for (int r = 0; r < 2; ++r) {
+                        b_rh[lane][r] = B.rh[r]; b_rl[lane][r] = B.rl[r];
+                        b_ih[lane][r] = B.ih[r]; b_il[lane][r] = B.il[r];
+                    }
+                }
+                float yr[32][4] = {}, yi[32][4] = {}, cr[32][4] = {}, ci[32][4] = {};
+                emu_mma(a_rl, b_rh, cr); emu_mma(a_il, b_rh, ci);
+                emu_mma(a_rh, b_rh, yr); emu_mma(a_ih, b_rh, yi);
+                emu_mma(a_rh, b_rl, cr); emu_mma(a_ih, b_rl, ci);
+                emu_mma(a_nih, b_ih, yr); emu_mma(a_rh, b_ih, yi);
+                emu_mma(a_nil, b_ih, cr); emu_mma(a_rl, b_ih, ci);
+                emu_mma(a_nih, b_il, cr); emu_mma(a_rh, b_il, ci);
+                for (int lane = 0; lane < 32; ++lane)
+                    for (int r = 0; r < 4; ++r) { yr[lane][r] += cr[lane][r]; yi[lane][r] += ci[lane][r]; }
+                for (int lane = 0; lane < 32; ++lane) {
+                    int t4 = lane & 3;
+                    float u0 = 1.0f / sc[8 * t4], u1 = 1.0f / sc[8 * t4 + 4];
+                    float r_[4] = {yr[lane][0] * u0, yr[lane][1] * u1, yr[lane][2] * u0, yr[lane][3] * u1};
+                    float i_[4] = {yi[lane][0] * u0, yi[lane][1] * u1, yi[lane][2] * u0, yi[lane][3] * u1};
+                    if (w * 32 + q * 8 + 2 * t4 + 1 < nbf) tc_write(sm, logR, lns, w, q, lane, r_, i_);
+                }
+            }
+    }
+}
+
+bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStream_t) {
+    if (sizeof(real_t) != 4 || log_tile != 12) {
+        set_error(6, "the split tensor-core form exists in the float library only");
+        return false;
+    }
+    using T = real_t;
+    using V = C2<T>;
+    constexpr int LT = 12, THREADS = (1 << LT) / 16;
+    g_launches++;
+    const TwTables<T>* tw = (const TwTables<T>*)a.tw;
+    const int logE = a.logR + a.logJ, J = 1 << a.logJ, E = 1 << logE;
+    g_smem_elems = (int)pass_smem_elems<T>(LT);
+    std::vector<V> sm(g_smem_elems);
+    std::vector<long long> lin(MAX_J), lout(MAX_J), lj(MAX_J);
+    std::vector<V> regs((size_t)THREADS * 16);
+    TileLines tl{lin.data(), lout.data(), lj.data()};
+    for (long long tile = 0; tile < ntiles; ++tile) {
+        const long long line0 = tile << a.logJ;
+        if (line0 >= a.nlines) continue;
+        for (auto& x : sm) x = mkc((T)NAN, (T)NAN);
+        for (int l = 0; l < J; ++l) line_setup(a, line0 + l, l, tl);
+        for (int e = 0; e < E; ++e) load_slot_commit<T>(a, tw, sm.data(), tl, e, load_slot_value<T, LD_C>(a, tw, tl, e));
+        int lns = 0;
+        for (int s = 0; s < a.nsub; ++s) {
+            int lr = a.sublog[s];
+            if (lr == 4) {
+                emu_tc_substage<THREADS>(sm, tw, a.logR, logE, lns);
+            } else {
+                for (int t = 0; t < THREADS; ++t) {
+                    V* v = &regs[(size_t)t * 16];
+                    if (lr == 3) substage_read<T, THREADS, 8, 3>(sm.data(), v, a.logR, logE, t);
+                    else if (lr == 2) substage_read<T, THREADS, 4, 2>(sm.data(), v, a.logR, logE, t);
+                    else substage_read<T, THREADS, 2, 1>(sm.data(), v, a.logR, logE, t);
+                }
+                for (int t = 0; t < THREADS; ++t) {
+                    V* v = &regs[(size_t)t * 16];
+                    if (lr == 3) substage_write<T, THREADS, 8, 3>(sm.data(), v, tw, a.logR, logE, lns, t);
+                    else if (lr == 2) substage_write<T, THREADS, 4, 2>(sm.data(), v, tw, a.logR, logE, lns, t);
+                    else substage_write<T, THREADS, 2, 1>(sm.data(), v, tw, a.logR, logE, lns, t);
+                }
+            }
+            lns += lr;
+        }
+        for (int e = 0; e < E; ++e) store_slot<T, ST_C>(a, tw, sm.data(), tl, e);
+    }
+    return true;
+}
 
 using EmuLean = void (*)(const PassArgs&, long long);
 static std::map<unsigned, EmuLean>& emu_lean_table() {

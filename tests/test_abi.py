@@ -75,3 +75,42 @@ def test_no_gpu_mkaux_returns_null():
     lib.notorious_fft_last_error.restype = ctypes.c_int
     assert not lib.notorious_fft_mkaux_dft_1d(16)
     assert lib.notorious_fft_last_error() != 0
+
+
+REF_HPP = "/root/reference/include/notorious_fft.hpp"
+
+
+@pytest.mark.skipif(not os.path.exists(REF_HPP), reason="reference sources not present")
+@pytest.mark.parametrize("single", [False, True], ids=["double", "float"])
+def test_reference_cpp_wrapper_compiles_against_this_header(tmp_path, single):
+    """The reference's C++17 wrapper (include/notorious_fft.hpp) builds
+    unchanged on top of include/notorious_fft.h and links against the library.
+    The wrapper is copied to a temporary directory at test time so that its
+    #include "notorious_fft.h" resolves to this repository's header."""
+    import shutil
+    shutil.copy(REF_HPP, tmp_path / "notorious_fft.hpp")
+    src = tmp_path / "app.cpp"
+    src.write_text(
+        '#include "notorious_fft.hpp"\n'
+        "int main() {\n"
+        "  auto a = notorious_fft::mkaux_dft_1d(64);\n"
+        "  std::vector<notorious_fft_cmpl> x(64), y(64);\n"
+        "  notorious_fft::dft(x.data(), y.data(), a);\n"
+        "  std::vector<notorious_fft::complex_t> v(64);\n"
+        "  auto w = notorious_fft::dft(v);\n"
+        "  std::vector<notorious_fft::real_t> r(64);\n"
+        "  auto z = notorious_fft::realdft(r);\n"
+        "  return (int)(w.size() + z.size()) == 0;\n"
+        "}\n")
+    lib = default_path(single)
+    if not os.path.exists(lib):
+        pytest.skip("library not built")
+    cmd = ["g++", "-std=c++17", "-c", "-I", str(tmp_path), "-I",
+           os.path.join(ROOT, "include"), str(src), "-o", str(tmp_path / "app.o")]
+    if single:
+        cmd.insert(2, "-DNOTORIOUS_FFT_SINGLE")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    r = subprocess.run(["g++", str(tmp_path / "app.o"), "-o", str(tmp_path / "app"), lib,
+                        "-Wl,-rpath," + os.path.dirname(lib)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]

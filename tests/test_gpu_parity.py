@@ -263,3 +263,40 @@ def test_float_library(lib_f, oracle_d, n):
                 assert rel_l2(a(k, xr), oracle_d.transform(k, xr.astype(np.float64))) <= tol(n, True), k
         with lib_f.mkaux("realdft", [n]) as a:
             assert rel_l2(a("realdft", xr), oracle_d.transform("realdft", xr.astype(np.float64))) <= tol(n, True)
+
+
+# ---------------------------------------------------------------------------
+# split tensor-core precision form (float library): configuration C3 shape
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n", [1 << 16, 4096, 1 << 14])
+def test_split_tc_form_error_per_transform(lib_f, oracle_d, n):
+    """FP32 storage, radix-16 DFTs as FP16 hi+lo tensor-core products: every
+    transform within 2e-6 relative L2 of the FP64 oracle, including a 10%
+    subset scaled by 1e4 (per-butterfly power-of-two scaling)."""
+    import torch
+    from notorious_fft import FORM_SPLIT_TC
+    B = 20
+    rng = np.random.default_rng(n)
+    x = (rng.standard_normal((B, n)) + 1j * rng.standard_normal((B, n)))
+    big = rng.choice(B, 2, replace=False)
+    x[big] *= 1e4
+    x = x.astype(np.complex64)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty_like(xd)
+    with lib_f.mkaux("dft", [n]) as a:
+        a.set_form(FORM_SPLIT_TC)
+        assert a.form == FORM_SPLIT_TC
+        for kind in ("dft", "invdft"):
+            a.batched(kind, xd, yd, B, n, n)
+            lib_f.synchronize()
+            y = yd.cpu().numpy()
+            ref = oracle_d.transform(kind, x.astype(np.complex128))
+            errs = [rel_l2(y[b], ref[b]) for b in range(B)]
+            assert max(errs) <= 2e-6, (kind, max(errs))
+
+
+def test_split_tc_form_rejected_by_double_library(lib_d):
+    from notorious_fft import FORM_SPLIT_TC, NotoriousFFTError
+    with lib_d.mkaux("dft", [4096]) as a:
+        with pytest.raises(NotoriousFFTError):
+            a.set_form(FORM_SPLIT_TC)
