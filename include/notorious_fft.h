@@ -223,6 +223,54 @@ int notorious_fft_get_form(const notorious_fft_aux* a);
 int notorious_fft_dft_noalloc(const notorious_fft_cmpl* x, notorious_fft_cmpl* y, int N, int howmany, int inverse,
                               void* stream);
 
+/* Ragged batches (no counterpart in the reference, whose callers loop over
+ * transforms one aux at a time, e.g. benchmarks/bench_mixed_sizes.c).  A
+ * batch is `count` independent 1-D transforms of mixed kinds
+ * (NOTORIOUS_FFT_KIND_*) and lengths, executed by ONE persistent GPU launch
+ * (captured in a CUDA graph) that works through a device queue of tiles.
+ * Transform i reads in + in_offsets[i] and writes out + out_offsets[i];
+ * offsets count notorious_fft_real elements (complex data: even offsets).
+ * NULL offsets select the packed layout: transforms back to back in index
+ * order, each starting at an even offset.  Every kind accepts power-of-two
+ * lengths; dft, invdft, realdft and dct2 accept any length >= 1 (Bluestein;
+ * realdft then returns floor(N/2)+1 bins, invdft scales by 1/N as the
+ * reference does).  Returns NULL on error (see notorious_fft_last_error). */
+typedef struct notorious_fft_batch notorious_fft_batch;
+notorious_fft_batch* notorious_fft_mkbatch(int count, const int* kinds, const int* Ns, const long long* in_offsets,
+                                           const long long* out_offsets);
+/* Input / output buffer sizes the batch needs, in notorious_fft_real. */
+long long notorious_fft_batch_in_size(const notorious_fft_batch* b);
+long long notorious_fft_batch_out_size(const notorious_fft_batch* b);
+/* Run the batch.  Device pointers: asynchronous on the current stream (check
+ * notorious_fft_batch_status afterwards).  Host pointers: staged, synchronous,
+ * returns the status.  Device buffers may be the same (in == out) only when
+ * every transform maps onto itself (equal offsets, length-preserving kinds);
+ * host buffers are staged and may always coincide.  Returns 0 or an error. */
+int notorious_fft_batch_execute(notorious_fft_batch* b, const notorious_fft_real* in, notorious_fft_real* out);
+/* Wait for the batch's last launch; NOTORIOUS_FFT_ERR_TIMEOUT if a bounded
+ * device wait gave up (the launch was abandoned and the output is invalid). */
+int notorious_fft_batch_status(notorious_fft_batch* b);
+/* Launch through a CUDA graph (default 1) or directly (0). */
+int notorious_fft_batch_set_graph(notorious_fft_batch* b, int enable);
+/* Queue statistics: items, tiles, device scratch bytes, persistent CTAs. */
+int notorious_fft_batch_info(const notorious_fft_batch* b, long long* items, long long* tiles,
+                             long long* scratch_bytes, int* ctas);
+void notorious_fft_free_batch(notorious_fft_batch* b);
+/* Test hook for the bounded waits: the next execution withholds one
+ * dependency (its counter is never published) and waits at most spin_limit
+ * polls, so the launch must end with NOTORIOUS_FFT_ERR_TIMEOUT. */
+int notorious_fft_batch_debug_withhold(notorious_fft_batch* b, long long spin_limit);
+
+/* Autotuner.  Times the executable pass splits of a power-of-two transform
+ * (kind, N) in the queue on this GPU, keeps the fastest, and stores it in the
+ * tune cache (a JSON file: $NOTORIOUS_FFT_TUNE_CACHE, default
+ * ~/.cache/notorious_fft/tune.json, keyed by GPU name + driver, precision,
+ * kind and N).  Later batches use the cached split.  Returns 0 or an error. */
+int notorious_fft_autotune(int kind, int N);
+/* The cached split for (kind, N): writes up to max_passes log2 radices and
+ * returns their count (0: none cached). */
+int notorious_fft_tune_lookup(int kind, int N, int* log2_radices, int max_passes);
+
 /* Library identification: precision of this build's notorious_fft_real
  * (8 or 4) and a short version string. */
 int notorious_fft_real_size(void);

@@ -26,7 +26,18 @@ LIB = os.path.join(HERE, "lib")
 BUILD = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu", "nfft_noalloc.cu", "nfft_cluster.cu", "nfft_tc.cu"] + [f"nfft_lean_s{k}.cu" for k in range(8)]
+QUEUE_BRANCHES = [f"nfft_queue_b{k}.cu" for k in range(4)]
+SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu", "nfft_noalloc.cu", "nfft_cluster.cu", "nfft_tc.cu",
+           "nfft_queue_build.cu", "nfft_queue_kernel.cu"] + QUEUE_BRANCHES + [f"nfft_lean_s{k}.cu" for k in range(8)]
+# The persistent queue kernel and its branch functions are relocatable device
+# code (linked by nvcc -dlink), so the branch units compile in parallel.  They
+# read data that other CTAs wrote earlier in the same launch: global loads
+# must be served by L2 (-dlcm=cg).  The branches get the kernel's register
+# budget (256 threads, 2 CTAs per SM).
+RDC_SOURCES = ["nfft_queue_kernel.cu"] + QUEUE_BRANCHES
+_QUEUE_FLAGS = ["-rdc=true", "-Xptxas", "-dlcm=cg"]
+SOURCE_FLAGS = {"nfft_queue_kernel.cu": _QUEUE_FLAGS}
+SOURCE_FLAGS.update({b: _QUEUE_FLAGS + ["-maxrregcount=128"] for b in QUEUE_BRANCHES})
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 PRECISIONS = {
     "d": ("libnotorious_fft.so", ["-DNFFT_REAL=double"]),
@@ -113,12 +124,22 @@ def build(only: str | None = None, jobs: int = 8, verbose_ptxas: bool = False) -
         futs = {}
         for p in precs:
             for s in SOURCES:
-                futs[(p, s)] = ex.submit(compile_one, s, p, PRECISIONS[p][1], verbose_ptxas)
+                futs[(p, s)] = ex.submit(compile_one, s, p, PRECISIONS[p][1] + SOURCE_FLAGS.get(s, []), verbose_ptxas)
         objs = {k: f.result() for k, f in futs.items()}
     for p in precs:
         name = PRECISIONS[p][0]
         out = os.path.join(LIB, name)
-        pobjs = [objs[(p, s)] for s in SOURCES]
+        # device link of the relocatable queue objects
+        robjs = [objs[(p, s)] for s in RDC_SOURCES]
+        dlink = os.path.join(BUILD, f"queue_dlink_{p}.o")
+        dcmd = [nvcc(), *ARCH, "-dlink", "-Xcompiler", "-fPIC", "-o", dlink, *robjs]
+        ddeps = robjs + [o + ".stamp" for o in robjs]
+        if not _fresh(dlink, ddeps, dcmd):
+            r = subprocess.run(dcmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"device link failed for {name}:\n{r.stderr}")
+            _stamp(dlink, ddeps, dcmd)
+        pobjs = [objs[(p, s)] for s in SOURCES] + [dlink]
         cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-Xlinker", "-Bsymbolic", "-Xlinker", "--no-undefined",
                "-o", out, *pobjs, "-lcudart_static", "-ldl", "-lrt", "-lpthread"]
         deps = pobjs + [o + ".stamp" for o in pobjs]

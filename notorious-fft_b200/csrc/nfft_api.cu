@@ -357,6 +357,66 @@ int notorious_fft_set_form(notorious_fft_aux* a, int form) {
 }
 int notorious_fft_get_form(const notorious_fft_aux* a) { return (a && a->plan) ? a->plan->form : -1; }
 
+// ---- ragged batches (persistent queue) -----------------------------------------
+notorious_fft_batch* notorious_fft_mkbatch(int count, const int* kinds, const int* Ns, const long long* in_offsets,
+                                           const long long* out_offsets) {
+    clear_error();
+    return batch_create_default(count, kinds, Ns, in_offsets, out_offsets);
+}
+long long notorious_fft_batch_in_size(const notorious_fft_batch* b) { return b ? batch_in_reals(b) : 0; }
+long long notorious_fft_batch_out_size(const notorious_fft_batch* b) { return b ? batch_out_reals(b) : 0; }
+
+int notorious_fft_batch_execute(notorious_fft_batch* b, const notorious_fft_real* in, notorious_fft_real* out) {
+    clear_error();
+    if (!b || ((!in || !out) && batch_in_reals(b) > 0)) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "NULL batch or buffer");
+        return NOTORIOUS_FFT_ERR_INVALID;
+    }
+    if (batch_in_reals(b) == 0) return 0;
+    const bool din = is_device_ptr(in), dout = is_device_ptr(out);
+    if (din != dout) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "batch input and output must both be device or both be host memory");
+        return NOTORIOUS_FFT_ERR_INVALID;
+    }
+    return din ? batch_run(b, in, out, t_stream) : batch_run_host(b, in, out, t_stream);
+}
+int notorious_fft_batch_status(notorious_fft_batch* b) {
+    clear_error();
+    if (!b) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "NULL batch");
+        return NOTORIOUS_FFT_ERR_INVALID;
+    }
+    return batch_status(b);
+}
+int notorious_fft_batch_set_graph(notorious_fft_batch* b, int enable) {
+    if (!b) return NOTORIOUS_FFT_ERR_INVALID;
+    batch_set_graph(b, enable);
+    return 0;
+}
+int notorious_fft_batch_info(const notorious_fft_batch* b, long long* items, long long* tiles, long long* scratch_bytes,
+                             int* ctas) {
+    if (!b) return NOTORIOUS_FFT_ERR_INVALID;
+    batch_info(b, items, tiles, scratch_bytes, ctas);
+    return 0;
+}
+void notorious_fft_free_batch(notorious_fft_batch* b) { batch_destroy(b); }
+int notorious_fft_batch_debug_withhold(notorious_fft_batch* b, long long spin_limit) {
+    if (!b) return NOTORIOUS_FFT_ERR_INVALID;
+    batch_withhold(b, spin_limit);
+    return 0;
+}
+
+int notorious_fft_autotune(int kind, int N) {
+    clear_error();
+    if (!current_ctx()) return last_error();
+    return autotune(kind, N, t_stream);
+}
+int notorious_fft_tune_lookup(int kind, int N, int* log2_radices, int max_passes) {
+    clear_error();
+    if (!log2_radices || max_passes < 1) return 0;
+    return tune_lookup(kind, N, log2_radices, max_passes);
+}
+
 int notorious_fft_real_size(void) { return (int)sizeof(real_t); }
 long long notorious_fft_launch_count(void) { return launch_count(); }
 const char* notorious_fft_version(void) { return "notorious-fft-b200 0.1 (sm_100a)"; }

@@ -48,12 +48,15 @@ template <typename V, typename S> NFFT_HD V cscale(V a, S s) { return mkc(a.x * 
 // ---------------------------------------------------------------------------
 // Global accesses with L2 policy.  hint 0: default; 1: streaming (user data
 // read or written once: evict first); 2: inter-pass scratch (stores kept in L2
-// with evict_last priority; the last read is followed by discard_l2).
+// with evict_last priority; the last read is followed by discard_l2); 3: data
+// written earlier in the same launch by other CTAs (loaded at L2, the point of
+// coherence, never from a possibly stale L1 line; stores as hint 2).
 // ---------------------------------------------------------------------------
 template <typename V>
 NFFT_HD V gload(const V* p, int hint) {
 #if defined(__CUDA_ARCH__)
     if (hint == 1 || hint == 2) return __ldcs(p);
+    if (hint == 3) return __ldcg(p);
     return *p;
 #else
     (void)hint;
@@ -64,7 +67,7 @@ NFFT_HD V gload(const V* p, int hint) {
 NFFT_HD void gstore(double2* p, double2 v, int hint) {
 #if defined(__CUDA_ARCH__)
     if (hint == 1) { __stcs(p, v); return; }
-    if (hint == 2) {
+    if (hint >= 2) {
         uint64_t pol;
         asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
         asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y), "l"(pol)
@@ -81,7 +84,7 @@ NFFT_HD void gstore(double2* p, double2 v, int hint) {
 NFFT_HD void gstore(float2* p, float2 v, int hint) {
 #if defined(__CUDA_ARCH__)
     if (hint == 1) { __stcs(p, v); return; }
-    if (hint == 2) {
+    if (hint >= 2) {
         uint64_t pol;
         asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
         asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol)

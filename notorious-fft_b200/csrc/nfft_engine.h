@@ -81,7 +81,11 @@ struct FftSchedule {
     int sub[4][MAX_SUB] = {};
 };
 // strided: the axis is not contiguous (every pass runs in column mode).
-FftSchedule make_schedule(int logL, bool strided);
+// max_tile: log2 of the largest tile (13: 512-thread kernels; 12: the queue).
+FftSchedule make_schedule(int logL, bool strided, int max_tile = 13);
+// Explicit pass radices (log2, execution order; 4096-point tiles).  False when
+// the split is not executable (radix too large for its tile, wrong sum).
+bool make_split_schedule(int logL, const int* plog, int npass, FftSchedule* out);
 FftSchedule reversed(const FftSchedule& s);
 
 // ---- one axis of a plan -------------------------------------------------------
@@ -95,10 +99,13 @@ struct AxisPlan {
     int logM = 0;
     cplx_t* chirp = nullptr;   // e^{-i pi k^2/n}, k < n
     cplx_t* filt = nullptr;    // FFT_M(conj chirp, wrapped) / M
+    cplx_t* post = nullptr;    // DCT-2 of any length: e^{-i pi q / 2n}, q < n (queue plans only)
     FftSchedule mfwd, minv;    // M-point forward schedule and its reverse
 };
 
 }  // namespace nfft
+
+struct notorious_fft_batch;   // a ragged batch (nfft_queue_build.cu)
 
 // The plan behind notorious_fft_aux::plan.
 struct notorious_fft_plan {
@@ -149,7 +156,34 @@ struct OpSpec {
     bool paired = false;   // st is ST_R / ST_T2 (needs whole lines or the unpack epilogue)
     int vjp = 0;           // adjoint weights of the real operators
     int tc = 0;            // split tensor-core radix-16 sub-stages (float library)
+    const void* post = nullptr;   // ST_BLUE_T2 post-twiddle table
 };
+
+// ---- launch recording (ragged-batch queue, nfft_queue.h) ---------------------
+// While recorder() is non-null on the calling thread, the planner records the
+// passes it would launch (queue branch key, arguments, tile count) instead of
+// launching them, and plans for the queue's 4096-point tiles.
+struct RecLaunch {
+    int op;                   // QOP_* key
+    PassArgs a;
+    long long ntiles;
+    const void* z = nullptr;  // unpack: packed spectrum and its line distance
+    long long zdist = 0;
+};
+struct Recorder {
+    std::vector<RecLaunch> launches;
+};
+Recorder*& recorder();
+bool queue_has_lean(int logR, int ci, int co, int ld, int st);
+// A 1-D plan of `kind` for the queue: 4096-point tiles, optional explicit pass
+// split of the inner power-of-two FFT (npass = 0: default schedule).  Any
+// length n >= 2 for dft / invdft, and for realdft / DCT-2 (Bluestein with
+// real-input operators when n is not a power of two); powers of two otherwise.
+notorious_fft_plan* plan_create_queue(int kind, int n, const int* plog, int npass);
+// Record the passes of `count` transforms of `kind` from in to out (recorder()
+// must be set).  Returns 0 on success.
+int plan_record(notorious_fft_plan* p, int kind, const void* in, void* out, long long count, long long idist,
+                long long odist);
 
 // One Stockham pass of an axis of length 2^logL (nfft_plan.cu).
 bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR, int tile,
@@ -166,7 +200,29 @@ bool launch_tiny(const real_t* x, real_t* y, long long howmany, long long inner,
                  int in_cplx, int out_cplx, double factor, cudaStream_t s);
 bool launch_init_tables(TwTables<real_t>* tw, cudaStream_t s);
 bool launch_chirp(cplx_t* chirp, cplx_t* bwrap, long long n, long long M, cudaStream_t s);
+// post[q] = e^{-i pi q / 2n}, q < n (FP64 sincospi)
+bool launch_post(cplx_t* post, long long n, cudaStream_t s);
 bool set_kernel_attributes();
+
+// Persistent queue kernel (nfft_queue_kernel.cu)
+struct QueueArgs;
+int queue_grid(const DeviceCtx* c);   // resident CTAs (0 on error)
+bool launch_queue(const QueueArgs& q, int grid, cudaStream_t s);
+
+// Ragged batches (nfft_queue_build.cu).  Offsets in reals, NULL: packed.
+notorious_fft_batch* batch_create_default(int count, const int* kinds, const int* Ns, const long long* in_off,
+                                          const long long* out_off);
+void batch_destroy(notorious_fft_batch* b);
+int batch_run(notorious_fft_batch* b, const void* din, void* dout, cudaStream_t s);        // device pointers, async
+int batch_run_host(notorious_fft_batch* b, const void* hin, void* hout, cudaStream_t s);   // host pointers, sync
+int batch_status(notorious_fft_batch* b);
+long long batch_in_reals(const notorious_fft_batch* b);
+long long batch_out_reals(const notorious_fft_batch* b);
+void batch_info(const notorious_fft_batch* b, long long* items, long long* tiles, long long* scratch, int* ctas);
+void batch_set_graph(notorious_fft_batch* b, int enable);
+void batch_withhold(notorious_fft_batch* b, long long spin_limit);
+int autotune(int kind, int n, cudaStream_t s);
+int tune_lookup(int kind, int n, int* plog, int max_passes);
 long long launch_count();
 void note_launch();
 

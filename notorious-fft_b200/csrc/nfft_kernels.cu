@@ -198,6 +198,23 @@ __global__ void chirp_kernel(cplx_t* chirp, cplx_t* bwrap, long long n, long lon
     }
 }
 
+// post[q] = e^{-i pi q / 2n}, q < n: FP64 sincospi of the fraction q / 2n
+// (the DCT-2 post-twiddle for lengths that are not powers of two).
+__global__ void post_kernel(cplx_t* post, long long n) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    double s, c;
+    sincospi((double)q / (double)(2 * n), &s, &c);
+    post[q] = mkc((real_t)c, (real_t)-s);
+}
+
+bool launch_post(cplx_t* post, long long n, cudaStream_t s) {
+    int threads = 256;
+    long long blocks = (n + threads - 1) / threads;
+    post_kernel<<<(unsigned)blocks, threads, 0, s>>>(post, n);
+    return cuda_ok(cudaGetLastError(), "post-twiddle kernel launch");
+}
+
 bool launch_chirp(cplx_t* chirp, cplx_t* bwrap, long long n, long long M, cudaStream_t s) {
     int threads = 256;
     long long blocks = (M + threads - 1) / threads;

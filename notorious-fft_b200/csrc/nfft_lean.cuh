@@ -105,7 +105,10 @@ struct Lean {
             const long long rs = a.in_estride << a.logNj;
             const C2<T>* src = (const C2<T>*)a.in + ln.bin + ln.j * a.in_estride + (long long)i * rs;
             const long long s16 = rs << (LOGR - 4);
-            if (a.hint_in) {
+            if (a.hint_in == 3) {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) v[m] = gload(src + m * s16, 3);
+            } else if (a.hint_in) {
 #pragma unroll
                 for (int m = 0; m < 16; ++m) v[m] = gload(src + m * s16, 1);
             } else {
@@ -269,17 +272,16 @@ constexpr size_t lean_smem_bytes() {
     return sizeof(C2<T>) * (size_t)L::SMEM_ELEMS + sizeof(LeanLine) * (size_t)L::J;
 }
 
+// One tile of a specialized pass (all threads of the CTA call it; uniform
+// early exit past the last line).
 template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
-__global__ void __launch_bounds__(1 << LOGT, (LOGT <= 7 ? 4 : (LOGT == 8 ? 2 : 1)))
-lean_pass_kernel(const PassArgs a) {
+__device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, unsigned char* smraw) {
     using L = Lean<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>;
     using V = C2<T>;
-    extern __shared__ __align__(16) unsigned char smraw[];
     V* sm = (V*)smraw;
     LeanLine* lines = (LeanLine*)(sm + L::SMEM_ELEMS);
     const TwTables<T>* tw = (const TwTables<T>*)a.tw;
     const int t = threadIdx.x;
-    const long long tile = (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x;
     const long long line0 = tile << L::LOGJ;
     if (line0 >= a.nlines) return;
     if (t < L::J) {
@@ -376,6 +378,14 @@ lean_pass_kernel(const PassArgs a) {
                                   [&](long long r) { return sm[NFFT_SM((lean_idx<false, LOGR, L::LOGJ>(ll, (int)r)))]; });
         }
     }
+}
+
+template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
+__global__ void __launch_bounds__(1 << LOGT, (LOGT <= 7 ? 4 : (LOGT == 8 ? 2 : 1)))
+lean_pass_kernel(const PassArgs a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    lean_tile<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>(a, (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x,
+                                                           smraw);
 }
 
 }  // namespace nfft

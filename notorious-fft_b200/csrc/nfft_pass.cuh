@@ -34,6 +34,8 @@ enum LoadOp : int {
     LD_T4 = 4,    // DCT-4/DST-4: premultiply (x[2n] +- i x[N-1-2n]) by e^{-i pi n/N}
     LD_BLUE = 5,  // Bluestein: chirp premultiply, zero pad beyond N
     LD_R2C = 6,   // realdft: N reals read pairwise as N/2 complex (any alignment / stride)
+    LD_BLUE_R = 7,   // Bluestein of N reals (realdft of any N): (x_p, 0) times the chirp
+    LD_BLUE_T2 = 8,  // Bluestein DCT-2 of any N: even / reversed-odd reorder of N reals, times the chirp
 };
 // Fused output operators.
 enum StoreOp : int {
@@ -44,7 +46,10 @@ enum StoreOp : int {
     ST_T4 = 4,    // DCT-4/DST-4 postmultiply
     ST_BLUE = 5,  // Bluestein: window [0, N), chirp postmultiply, scale
     ST_C2R = 6,   // invrealdft: complex element written as two reals (any alignment / stride)
+    ST_BLUE_R = 7,   // Bluestein realdft of any N: bins 0 .. N/2 of the windowed, chirped output
+    ST_BLUE_T2 = 8,  // Bluestein DCT-2 of any N: y_q = 2 Re(e^{-i pi q/2N} V_q), q < N
 };
+constexpr int NUM_LOAD_OPS = 9, NUM_STORE_OPS = 9;
 
 constexpr int MAX_LINE_DIMS = 4;
 constexpr int MAX_SUB = 4;
@@ -78,6 +83,12 @@ struct PassArgs {
     int hint_in, hint_out;   // L2 policy of the complex input / output (gload / gstore)
     int discard_in;          // input is scratch read for the last time: drop its L2 lines
     int tw_mode;             // pass pre-twiddles: 0 product tree, 1 chained products, 2 table lookups
+    // Ragged batches: line dim tab_dim takes its input / output offset from a
+    // per-index table (elements of the array type) instead of index * stride.
+    const long long* in_tab;
+    const long long* out_tab;
+    int tab_dim;
+    const void* post;        // Bluestein DCT-2 post-twiddle e^{-i pi q / 2N}, q < N (C2<T>)
 };
 
 // Shared-memory index with one padding element every 16 (breaks the
@@ -96,6 +107,14 @@ NFFT_HD C2<T> load_elem(const PassArgs& a, const TwTables<T>* tw, long long base
         V v = NFFT_GLD(&((const V*)a.in)[base + p * a.in_estride]);
         if (a.conj_in) v.y = -v.y;
         return cmul(v, NFFT_GLD(&((const V*)a.chirp)[p]));
+    } else if constexpr (OP == LD_BLUE_R || OP == LD_BLUE_T2) {
+        if (p >= a.N) return mkc((T)0, (T)0);
+        const T* x = (const T*)a.in + base;
+        const long long es = a.in_estride;
+        T r;
+        if constexpr (OP == LD_BLUE_R) r = NFFT_GLD(&x[p * es]);
+        else r = (p < (a.N + 1) / 2) ? NFFT_GLD(&x[(2 * p) * es]) : NFFT_GLD(&x[(2 * a.N - 1 - 2 * p) * es]);
+        return cscale(NFFT_GLD(&((const V*)a.chirp)[p]), r);
     } else if constexpr (OP == LD_R2C) {
         const T* x = (const T*)a.in + base;
         const long long es = a.in_estride;
@@ -190,6 +209,18 @@ NFFT_HD void store_elem(const PassArgs& a, const TwTables<T>* tw, long long base
         if (a.conj_out) v.y = -v.y;
         if (a.scale != 1.0) v = cscale(v, (T)a.scale);
         NFFT_GST(&((V*)a.out)[base + q * a.out_estride], v);
+    } else if constexpr (OP == ST_BLUE_R) {
+        if (q > a.N / 2) return;
+        v = cmul(cconj(v), NFFT_GLD(&((const V*)a.chirp)[q]));
+        if (a.scale != 1.0) v = cscale(v, (T)a.scale);
+        NFFT_GST(&((V*)a.out)[base + q * a.out_estride], v);
+    } else if constexpr (OP == ST_BLUE_T2) {
+        if (q >= a.N) return;
+        v = cmul(cconj(v), NFFT_GLD(&((const V*)a.chirp)[q]));
+        const V w = NFFT_GLD(&((const V*)a.post)[q]);
+        T y = (T)2 * (v.x * w.x - v.y * w.y);
+        if (a.scale != 1.0) y = (T)(y * a.scale);
+        NFFT_GST(&((T*)a.out)[base + q * a.out_estride], y);
     } else if constexpr (OP == ST_T3) {
         // real output t[2q], t[2q+1] of the inverse FFT -> y[2i] = t_i, y[N-1-2i] = +-t_{N/2+i}
         v = cconj(v);
@@ -310,8 +341,12 @@ NFFT_HD void line_setup(const PassArgs& a, long long lam, int l, TileLines tl) {
         for (int d = 0; d < a.ndims; ++d) {
             long long c = rem % a.cnt[d];
             rem /= a.cnt[d];
-            if (d == a.jpos) j = c;
-            else { bin += c * a.istr[d]; bout += c * a.ostr[d]; }
+            if (d == a.jpos) {
+                j = c;
+            } else {
+                bin += (d == a.tab_dim && a.in_tab) ? NFFT_GLD(&a.in_tab[c]) : c * a.istr[d];
+                bout += (d == a.tab_dim && a.out_tab) ? NFFT_GLD(&a.out_tab[c]) : c * a.ostr[d];
+            }
         }
     } else {
         j = -1;
@@ -472,12 +507,12 @@ template <typename T> constexpr size_t pass_smem_bytes(int log_tile) {
     return sizeof(C2<T>) * pass_smem_elems<T>(log_tile) + (size_t)MAX_J * 3 * sizeof(long long);
 }
 
+// One tile of the generic pass (all threads of the CTA call it; uniform early
+// exit past the last line).
 template <typename T, int LOG_TILE, int LOAD, int STORE>
-__global__ void __launch_bounds__((1 << LOG_TILE) / 16)
-pass_kernel(const PassArgs a) {
+__device__ __forceinline__ void pass_tile(const PassArgs& a, long long tile, unsigned char* smraw) {
     using V = C2<T>;
     constexpr int THREADS = (1 << LOG_TILE) / 16;
-    extern __shared__ __align__(16) unsigned char smraw[];
     V* sm = (V*)smraw;
     TileLines tl;
     tl.in = (long long*)(sm + pass_smem_elems<T>(LOG_TILE));
@@ -488,7 +523,6 @@ pass_kernel(const PassArgs a) {
     const int tid = threadIdx.x;
     const int logE = a.logR + a.logJ;
     const int J = 1 << a.logJ, E = 1 << logE;
-    const long long tile = (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x;
     const long long line0 = tile << a.logJ;
     if (line0 >= a.nlines) return;
 
@@ -531,6 +565,13 @@ pass_kernel(const PassArgs a) {
     }
 }
 
+template <typename T, int LOG_TILE, int LOAD, int STORE>
+__global__ void __launch_bounds__((1 << LOG_TILE) / 16)
+pass_kernel(const PassArgs a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    pass_tile<T, LOG_TILE, LOAD, STORE>(a, (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x, smraw);
+}
+
 // Paired-unpack epilogue for transforms whose packed spectrum needed more
 // than one pass: reads Z (M complex per line, contiguous, line distance zdist)
 // and writes realdft bins or DCT-2/DST-2 outputs.
@@ -544,10 +585,24 @@ NFFT_HD void unpack_item(const PassArgs& a, const TwTables<T>* tw, const C2<T>* 
     for (int d = 0; d < a.ndims; ++d) {
         long long c = rem % a.cnt[d];
         rem /= a.cnt[d];
-        bout += c * a.ostr[d];
+        bout += (d == a.tab_dim && a.out_tab) ? NFFT_GLD(&a.out_tab[c]) : c * a.ostr[d];
     }
     const C2<T>* zl = Z + line * zdist;
     unpack_pair<T, STORE>(a, tw, bout, k, M, [&](long long i) { return NFFT_GLD(&zl[i]); });
+}
+
+// Work items of one unpack tile: chunk `chunk` (UNPACK_TILE items) of one line.
+constexpr int UNPACK_TILE = 2048;
+NFFT_HD long long unpack_per_line(const PassArgs& a) { return (a.N / 2) >= 2 ? a.N / 4 : 1; }
+NFFT_HD long long unpack_tiles_per_line(const PassArgs& a) {
+    return (unpack_per_line(a) + UNPACK_TILE - 1) / UNPACK_TILE;
+}
+NFFT_HD void unpack_tile_range(const PassArgs& a, long long tile, long long& w0, long long& w1) {
+    const long long per = unpack_per_line(a), tpl = unpack_tiles_per_line(a);
+    const long long line = tile / tpl, chunk = tile - line * tpl;
+    w0 = line * per + chunk * UNPACK_TILE;
+    w1 = w0 + UNPACK_TILE;
+    if (w1 > (line + 1) * per) w1 = (line + 1) * per;
 }
 
 template <typename T, int STORE>

@@ -7,6 +7,7 @@
 #include <algorithm>
 
 #include "nfft_engine.h"
+#include "nfft_queue.h"
 
 namespace nfft {
 
@@ -127,10 +128,9 @@ static void split_sub(int logR, int* nsub, int* sub) {
     *nsub = n;
 }
 
-FftSchedule make_schedule(int logL, bool strided) {
+FftSchedule make_schedule(int logL, bool strided, int max_tile) {
     FftSchedule s;
     s.logL = logL;
-    const int max_tile = 13;
     const int jmin = log_jmin();
     if (!strided && logL <= max_tile) {
         s.npass = 1;
@@ -143,10 +143,29 @@ FftSchedule make_schedule(int logL, bool strided) {
         s.npass = np;
         int base = logL / np, extra = logL % np;
         for (int i = 0; i < np; ++i) s.plog[i] = base + (i < extra ? 1 : 0);
-        for (int i = 0; i < np; ++i) s.tile[i] = (s.plog[i] + jmin + 1 <= 12) ? 12 : 13;
+        for (int i = 0; i < np; ++i) s.tile[i] = std::min(max_tile, (s.plog[i] + jmin + 1 <= 12) ? 12 : 13);
     }
     for (int i = 0; i < s.npass; ++i) split_sub(s.plog[i], &s.nsub[i], s.sub[i]);
     return s;
+}
+
+bool make_split_schedule(int logL, const int* plog, int npass, FftSchedule* out) {
+    if (npass < 1 || npass > 4) return false;
+    FftSchedule s;
+    s.logL = logL;
+    s.npass = npass;
+    int sum = 0;
+    for (int i = 0; i < npass; ++i) {
+        const int lim = npass == 1 ? 12 : 12 - log_jmin();   // column passes keep >= jmin lines per tile
+        if (plog[i] < 1 || plog[i] > lim) return false;
+        s.plog[i] = plog[i];
+        s.tile[i] = 12;
+        split_sub(plog[i], &s.nsub[i], s.sub[i]);
+        sum += plog[i];
+    }
+    if (sum != logL) return false;
+    *out = s;
+    return true;
 }
 
 FftSchedule reversed(const FftSchedule& s) {
@@ -189,7 +208,23 @@ static bool lean_disabled() {
     return v == 1;
 }
 
+Recorder*& recorder() {
+    static thread_local Recorder* r = nullptr;
+    return r;
+}
+
+bool queue_has_lean(int logR, int ci, int co, int ld, int st) {
+    const int k = qop_lean(logR, ci, co, ld, st);
+#define X(R, CI, CO, LD, ST) \
+    if (k == qop_lean(R, CI, CO, LD, ST)) return true;
+    NFFT_QUEUE_LEAN(X)
+#undef X
+    return false;
+}
+
 static size_t scratch_cap_bytes() {
+    // a recorded (queue) bucket runs in one piece: its scratch is its own
+    if (recorder()) return (size_t)1 << 62;
     static size_t cap = 0;
     if (!cap) {
         const char* e = getenv("NOTORIOUS_FFT_SCRATCH_MB");
@@ -326,6 +361,33 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
         set_error(6, "pass radix 2^%d exceeds tile 2^%d", logR, tile);
         return false;
     }
+    a.post = op.post;
+    if (Recorder* rec = recorder()) {
+        // queue form: a branch of the persistent 256-thread kernel.  Scratch
+        // written earlier in the same launch is read through L2 (hint 3).
+        if (in_scratch || out_scratch) {
+            a.hint_in = in_scratch ? 3 : 1;
+            a.hint_out = out_scratch ? 2 : 1;
+            a.discard_in = in_scratch ? 1 : 0;
+        }
+        const int ci = a.in_row ? 0 : 1, co = a.out_row ? 0 : 1;
+        RecLaunch r;
+        if (!mid && logR >= 4 && !lean_disabled() && queue_has_lean(logR, ci, co, ldop, stop)) {
+            a.logJ = QUEUE_LOGT + 4 - logR;
+            r.op = qop_lean(logR, ci, co, ldop, stop);
+        } else {
+            if (tile != QUEUE_LOG_TILE) {
+                set_error(6, "queue pass of radix 2^%d needs a 2^%d tile", logR, tile);
+                return false;
+            }
+            a.logJ = logJ;
+            r.op = qop_gen(ldop, stop);
+        }
+        r.a = a;
+        r.ntiles = (a.nlines + (1ll << a.logJ) - 1) >> a.logJ;
+        rec->launches.push_back(r);
+        return true;
+    }
     // split tensor-core form: radix-16 sub-stages on the tensor cores
     if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR >= 4 && tile == 12 && logJ == 12 - logR) {
         a.logJ = logJ;
@@ -388,7 +450,7 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
     const int np = sch.npass;
     // One transform per thread-block cluster: no inter-pass scratch at all.
     if (np > 1 && !strided && !op.tc && op.ld == LD_C && op.st == ST_C && src.nb <= 1 && dst.nb <= 1 &&
-        cluster_available(logL)) {
+        !recorder() && cluster_available(logL)) {
         const int lr1 = cluster_logr1(logL), lr2 = logL - lr1;
         PassArgs a1, a2;
         fill_common(a1, c);
@@ -480,6 +542,17 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
                 a.cnt[0] = 1;
                 a.ostr[0] = 0;
             }
+            if (Recorder* rec = recorder()) {
+                RecLaunch r;
+                r.op = qop_unpack(op.st);
+                a.nlines = vs.lines();
+                r.a = a;
+                r.ntiles = a.nlines * unpack_tiles_per_line(a);
+                r.z = cur.ptr;
+                r.zdist = L;
+                rec->launches.push_back(r);
+                continue;
+            }
             if (!launch_unpack(a, op.st, (const cplx_t*)cur.ptr, L, vs.lines(), s)) return false;
         }
     }
@@ -487,13 +560,17 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
 }
 
 // Bluestein for a complex axis of length n (not a power of two).
+// ld / st: LD_BLUE / ST_BLUE for complex data; the real-input operators
+// (LD_BLUE_R, LD_BLUE_T2 / ST_BLUE_R, ST_BLUE_T2) give realdft and DCT-2 of
+// any length (queue plans).
 static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisPlan& ax, View src, View dst,
-                               int inverse, double scale, cudaStream_t s) {
+                               int inverse, double scale, cudaStream_t s, int ld = LD_BLUE, int st = ST_BLUE) {
     const int logM = ax.logM;
     const long long M = 1ll << logM;
     OpSpec op;
-    op.ld = LD_BLUE;
-    op.st = ST_BLUE;
+    op.ld = ld;
+    op.st = st;
+    op.post = ax.post;
     op.conj_in = inverse;
     op.conj_out = inverse;
     op.scale = scale;
@@ -521,9 +598,11 @@ static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const 
         long long cn = std::min(chunk, outer - o0);
         View vs = src, vd = dst;
         if (src.nb > 0) {
-            vs.ptr = (cplx_t*)src.ptr + o0 * src.str[src.nb - 1];
+            const size_t ib = ld == LD_BLUE ? sizeof(cplx_t) : sizeof(real_t);
+            const size_t ob = st == ST_BLUE_T2 ? sizeof(real_t) : sizeof(cplx_t);
+            vs.ptr = (char*)src.ptr + (size_t)(o0 * src.str[src.nb - 1]) * ib;
             vs.cnt[src.nb - 1] = cn;
-            vd.ptr = (cplx_t*)dst.ptr + o0 * dst.str[dst.nb - 1];
+            vd.ptr = (char*)dst.ptr + (size_t)(o0 * dst.str[dst.nb - 1]) * ob;
             vd.cnt[dst.nb - 1] = cn;
         }
         View cur = vs;
@@ -568,14 +647,14 @@ static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const 
 // ---------------------------------------------------------------------------
 // plans
 // ---------------------------------------------------------------------------
-static bool build_axis(notorious_fft_plan* p, const DeviceCtx* c, AxisPlan& ax, int n, int family) {
+static bool build_axis(notorious_fft_plan* p, const DeviceCtx* c, AxisPlan& ax, int n, int family, int max_tile = 13) {
     ax.n = n;
     ax.pow2 = is_pow2(n);
     ax.logn = ilog2(n);
     if (ax.pow2) {
         int logL = (family == FAM_DFT) ? ax.logn : std::max(0, ax.logn - 1);
-        ax.fft_contig = make_schedule(logL, false);
-        ax.fft_strided = make_schedule(logL, true);
+        ax.fft_contig = make_schedule(logL, false, max_tile);
+        ax.fft_strided = make_schedule(logL, true, max_tile);
         return true;
     }
     if (family != FAM_DFT) {
@@ -585,7 +664,7 @@ static bool build_axis(notorious_fft_plan* p, const DeviceCtx* c, AxisPlan& ax, 
     long long M = 1;
     while (M < 2ll * n - 1) M <<= 1;
     ax.logM = ilog2(M);
-    ax.mfwd = make_schedule(ax.logM, false);
+    ax.mfwd = make_schedule(ax.logM, false, max_tile);
     ax.minv = reversed(ax.mfwd);
     if (!cuda_ok(cudaMalloc((void**)&ax.chirp, sizeof(cplx_t) * (size_t)n), "cudaMalloc(chirp)")) return false;
     if (!cuda_ok(cudaMalloc((void**)&ax.filt, sizeof(cplx_t) * (size_t)M), "cudaMalloc(filter)")) return false;
@@ -659,6 +738,7 @@ void plan_destroy(notorious_fft_plan* p) {
     for (auto& ax : p->axes) {
         if (ax.chirp) cudaFree(ax.chirp);
         if (ax.filt) cudaFree(ax.filt);
+        if (ax.post) cudaFree(ax.post);
     }
     for (int i = 0; i < 2; ++i)
         if (p->scratch[i]) cudaFree(p->scratch[i]);
@@ -903,6 +983,73 @@ int plan_execute(notorious_fft_plan* p, int okind, const void* in, void* out, lo
         }
     }
     if (!ok) return last_error() ? last_error() : 4;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// ragged-batch queue plans (nfft_queue_build.cu)
+// ---------------------------------------------------------------------------
+notorious_fft_plan* plan_create_queue(int kind, int n, const int* plog, int npass) {
+    if (n < 2) {
+        set_error(1, "queue plans need n >= 2 (got %d)", n);
+        return nullptr;
+    }
+    const bool pow2 = is_pow2(n);
+    if (!pow2 && kind != K_DFT && kind != K_INVDFT && kind != K_REALDFT && kind != K_DCT2) {
+        set_error(6, "kind %d of length %d: only dft, invdft, realdft and dct2 accept lengths that are not powers of two",
+                  kind, n);
+        return nullptr;
+    }
+    DeviceCtx* c = current_ctx();
+    if (!c) return nullptr;
+    notorious_fft_plan* p = new notorious_fft_plan();
+    p->family = pow2 ? family_of(kind) : FAM_DFT;
+    p->device = c->device;
+    p->dims.assign(1, n);
+    p->axes.resize(1);
+    AxisPlan& ax = p->axes[0];
+    if (!build_axis(p, c, ax, n, p->family, 12)) {
+        plan_destroy(p);
+        return nullptr;
+    }
+    if (npass > 0 && pow2) {
+        FftSchedule sch;
+        if (!make_split_schedule(ax.fft_contig.logL, plog, npass, &sch)) {
+            set_error(1, "pass split does not fit a 2^%d transform", ax.fft_contig.logL);
+            plan_destroy(p);
+            return nullptr;
+        }
+        ax.fft_contig = sch;
+    }
+    if (!pow2 && kind == K_DCT2) {
+        bool ok = cuda_ok(cudaMalloc((void**)&ax.post, sizeof(cplx_t) * (size_t)n), "cudaMalloc(post-twiddle)") &&
+                  launch_post(ax.post, n, 0) && cuda_ok(cudaDeviceSynchronize(), "post-twiddle table");
+        if (!ok) {
+            plan_destroy(p);
+            return nullptr;
+        }
+    }
+    return p;
+}
+
+int plan_record(notorious_fft_plan* p, int kind, const void* in, void* out, long long count, long long idist,
+                long long odist) {
+    if (!recorder()) {
+        set_error(1, "plan_record needs an active recorder");
+        return 1;
+    }
+    const AxisPlan& ax = p->axes[0];
+    if (ax.pow2 || kind == K_DFT || kind == K_INVDFT) return plan_execute(p, kind, in, out, count, idist, odist, 0, 0);
+    // realdft / DCT-2 of a length that is not a power of two: N-point complex
+    // Bluestein of the (reordered) real input with the real-output epilogue
+    DeviceCtx* c = device_ctx(p->device);
+    if (!c) return last_error();
+    std::vector<long long> Din(1, ax.n), Dout(1, kind == K_REALDFT ? ax.n / 2 + 1 : ax.n);
+    View src = axis_view((void*)in, Din, 0, count, idist);
+    View dst = axis_view(out, Dout, 0, count, odist);
+    const int ld = kind == K_REALDFT ? LD_BLUE_R : LD_BLUE_T2;
+    const int st = kind == K_REALDFT ? ST_BLUE_R : ST_BLUE_T2;
+    if (!run_bluestein_axis(p, c, ax, src, dst, 0, 1.0, 0, ld, st)) return last_error() ? last_error() : 4;
     return 0;
 }
 

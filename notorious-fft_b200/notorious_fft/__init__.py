@@ -39,7 +39,11 @@ EXTENSION_SYMBOLS = (
     + ["notorious_fft_vjp_batched", "notorious_fft_execute_batched", "notorious_fft_last_error",
        "notorious_fft_last_error_string", "notorious_fft_clear_error", "notorious_fft_set_stream",
        "notorious_fft_get_stream", "notorious_fft_synchronize", "notorious_fft_set_form", "notorious_fft_get_form",
-       "notorious_fft_real_size", "notorious_fft_version", "notorious_fft_launch_count"]
+       "notorious_fft_real_size", "notorious_fft_version", "notorious_fft_launch_count",
+       "notorious_fft_dft_noalloc", "notorious_fft_mkbatch", "notorious_fft_batch_in_size",
+       "notorious_fft_batch_out_size", "notorious_fft_batch_execute", "notorious_fft_batch_status",
+       "notorious_fft_batch_set_graph", "notorious_fft_batch_info", "notorious_fft_free_batch",
+       "notorious_fft_batch_debug_withhold", "notorious_fft_autotune", "notorious_fft_tune_lookup"]
 )
 
 
@@ -88,6 +92,24 @@ class Library:
         L.notorious_fft_real_size.restype = I
         L.notorious_fft_version.restype = ctypes.c_char_p
         L.notorious_fft_launch_count.restype = ctypes.c_longlong
+        LL = ctypes.c_longlong
+        PLL = ctypes.POINTER(LL)
+        L.notorious_fft_mkbatch.argtypes = [I, V, V, V, V]
+        L.notorious_fft_mkbatch.restype = V
+        L.notorious_fft_batch_in_size.argtypes = [V]
+        L.notorious_fft_batch_in_size.restype = LL
+        L.notorious_fft_batch_out_size.argtypes = [V]
+        L.notorious_fft_batch_out_size.restype = LL
+        L.notorious_fft_batch_execute.argtypes, L.notorious_fft_batch_execute.restype = [V, V, V], I
+        L.notorious_fft_batch_status.argtypes, L.notorious_fft_batch_status.restype = [V], I
+        L.notorious_fft_batch_set_graph.argtypes, L.notorious_fft_batch_set_graph.restype = [V, I], I
+        L.notorious_fft_batch_info.argtypes = [V, PLL, PLL, PLL, ctypes.POINTER(I)]
+        L.notorious_fft_batch_info.restype = I
+        L.notorious_fft_free_batch.argtypes, L.notorious_fft_free_batch.restype = [V], None
+        L.notorious_fft_batch_debug_withhold.argtypes = [V, LL]
+        L.notorious_fft_batch_debug_withhold.restype = I
+        L.notorious_fft_autotune.argtypes, L.notorious_fft_autotune.restype = [I, I], I
+        L.notorious_fft_tune_lookup.argtypes, L.notorious_fft_tune_lookup.restype = [I, I, ctypes.POINTER(I), I], I
         self.real_size = L.notorious_fft_real_size()
         self.single = self.real_size == 4
         self.rdt = np.float32 if self.single else np.float64
@@ -118,6 +140,19 @@ class Library:
             code, msg = self.last_error()
             raise NotoriousFFTError(f"mkaux_{fam}{tuple(dims)} failed ({code}: {msg})")
         return Aux(self, ptr, fam, tuple(dims))
+
+    def mkbatch(self, kinds: Sequence[str], Ns: Sequence[int], in_offsets=None, out_offsets=None) -> "Batch":
+        """A ragged batch (one persistent launch for all transforms)."""
+        return Batch(self, kinds, Ns, in_offsets, out_offsets)
+
+    def autotune(self, kind: str, n: int) -> None:
+        if self.lib.notorious_fft_autotune(KIND_CODE[kind], int(n)):
+            self.check()
+
+    def tune_lookup(self, kind: str, n: int) -> list:
+        buf = (ctypes.c_int * 4)()
+        k = self.lib.notorious_fft_tune_lookup(KIND_CODE[kind], int(n), buf, 4)
+        return [buf[i] for i in range(min(k, 4))]
 
     def mkaux_raw(self, fam: str, dims: Sequence[int]):
         """The raw pointer (or None) -- mirrors the C convention of returning NULL."""
@@ -260,6 +295,79 @@ def _call_vjp_batched(self, kind, g, gx, aux, howmany, idist, odist):
 
 
 Library._call_vjp_batched = _call_vjp_batched
+
+
+class Batch:
+    """A ragged batch: transform i is kinds[i] of length Ns[i], reading
+    in[in_offsets[i]:] and writing out[out_offsets[i]:] (offsets in reals;
+    None: packed layout).  Buffers are flat real arrays (numpy or CUDA torch)
+    of at least in_size / out_size reals."""
+
+    def __init__(self, lib: Library, kinds, Ns, in_offsets=None, out_offsets=None):
+        self.L = lib
+        self.kinds = [KIND_CODE[k] if isinstance(k, str) else int(k) for k in kinds]
+        self.Ns = [int(n) for n in Ns]
+        count = len(self.kinds)
+        ka = np.ascontiguousarray(self.kinds, dtype=np.int32)
+        na = np.ascontiguousarray(self.Ns, dtype=np.int32)
+        ia = None if in_offsets is None else np.ascontiguousarray(in_offsets, dtype=np.int64)
+        oa = None if out_offsets is None else np.ascontiguousarray(out_offsets, dtype=np.int64)
+        self.ptr = lib.lib.notorious_fft_mkbatch(count, ka.ctypes.data, na.ctypes.data,
+                                                 None if ia is None else ia.ctypes.data,
+                                                 None if oa is None else oa.ctypes.data)
+        if not self.ptr:
+            code, msg = lib.last_error()
+            raise NotoriousFFTError(f"mkbatch failed ({code}: {msg})")
+        self.in_size = lib.lib.notorious_fft_batch_in_size(self.ptr)
+        self.out_size = lib.lib.notorious_fft_batch_out_size(self.ptr)
+
+    def free(self):
+        if getattr(self, "ptr", None):
+            self.L.lib.notorious_fft_free_batch(self.ptr)
+            self.ptr = None
+
+    __del__ = free
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
+
+    def execute(self, x, y):
+        """Run the batch; host arrays return when done, device tensors are asynchronous."""
+        L = self.L
+        hooks = []
+        if L._register is not None:
+            for a in (x, y):
+                if isinstance(a, np.ndarray):
+                    L._register(a.ctypes.data, a.nbytes)
+                    hooks.append(a.ctypes.data)
+        try:
+            rc = L.lib.notorious_fft_batch_execute(self.ptr, L._ptr(x), L._ptr(y))
+        finally:
+            for h in hooks:
+                L._unregister(h)
+        if rc:
+            L.check()
+            raise NotoriousFFTError(f"batch execute returned {rc}")
+        return y
+
+    def status(self) -> int:
+        return self.L.lib.notorious_fft_batch_status(self.ptr)
+
+    def set_graph(self, on: bool) -> None:
+        self.L.lib.notorious_fft_batch_set_graph(self.ptr, 1 if on else 0)
+
+    def withhold(self, spin_limit: int) -> None:
+        self.L.lib.notorious_fft_batch_debug_withhold(self.ptr, int(spin_limit))
+
+    def info(self) -> dict:
+        it, tl, sc = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        ctas = ctypes.c_int()
+        self.L.lib.notorious_fft_batch_info(self.ptr, ctypes.byref(it), ctypes.byref(tl), ctypes.byref(sc),
+                                            ctypes.byref(ctas))
+        return {"items": it.value, "tiles": tl.value, "scratch_bytes": sc.value, "ctas": ctas.value}
 
 
 _LIBS: dict = {}

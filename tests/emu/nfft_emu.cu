@@ -79,6 +79,23 @@ cudaError_t MemcpyAsync(void* d, const void* s, size_t b, cudaMemcpyKind, cudaSt
     memmove(d, s, b);
     return cudaSuccess;
 }
+// Synchronous copy between library-internal host memory and device memory:
+// only the device side is checked.
+cudaError_t Memcpy(void* d, const void* s, size_t b, cudaMemcpyKind k) {
+    if (k != cudaMemcpyHostToDevice) check_range(s, b, "memcpy src");
+    if (k != cudaMemcpyDeviceToHost) check_range(d, b, "memcpy dst");
+    memmove(d, s, b);
+    return cudaSuccess;
+}
+cudaError_t MemsetAsync(void* d, int v, size_t b, cudaStream_t = 0) {
+    check_range(d, b, "memset");
+    memset(d, v, b);
+    return cudaSuccess;
+}
+cudaError_t DriverGetVersion(int* v) {
+    *v = 0;
+    return cudaSuccess;
+}
 cudaError_t Memcpy2DAsync(void* d, size_t dp, const void* s, size_t sp, size_t w, size_t h, cudaMemcpyKind k,
                           cudaStream_t st = 0) {
     for (size_t r = 0; r < h; ++r) MemcpyAsync((char*)d + r * dp, (const char*)s + r * sp, w, k, st);
@@ -122,6 +139,11 @@ cudaError_t EventCreateWithFlags(cudaEvent_t* e, unsigned) {
     *e = (cudaEvent_t)&dummy[(n++) & 255];
     return cudaSuccess;
 }
+cudaError_t EventCreate(cudaEvent_t* e) { return EventCreateWithFlags(e, 0); }
+cudaError_t EventElapsedTime(float* ms, cudaEvent_t, cudaEvent_t) {
+    *ms = 1.0f;
+    return cudaSuccess;
+}
 const char* ErrorString(cudaError_t) { return "emulated CUDA error"; }
 }  // namespace emu
 
@@ -147,6 +169,11 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 #define cudaFree emu::Free
 #define cudaMemcpyAsync emu::MemcpyAsync
 #define cudaMemcpy2DAsync emu::Memcpy2DAsync
+#define cudaMemcpy emu::Memcpy
+#define cudaMemsetAsync emu::MemsetAsync
+#define cudaDriverGetVersion emu::DriverGetVersion
+#define cudaEventCreate emu::EventCreate
+#define cudaEventElapsedTime emu::EventElapsedTime
 #define cudaStreamSynchronize(s) emu::Ok()
 #define cudaDeviceSynchronize() emu::Ok()
 #define cudaSetDevice(d) emu::Ok()
@@ -165,10 +192,12 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 
 #include "../../notorious-fft_b200/csrc/nfft_plan.cu"
 #include "../../notorious-fft_b200/csrc/nfft_api.cu"
+#include "../../notorious-fft_b200/csrc/nfft_queue_build.cu"
 #include "../../notorious-fft_b200/csrc/nfft_lean.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_lean_list.h"
 #include "../../notorious-fft_b200/csrc/nfft_cluster.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_tc.cuh"
+#include "../../notorious-fft_b200/csrc/nfft_queue.h"
 
 // ---------------------------------------------------------------------------
 // emulated launches: the kernels' phase functions for every thread
@@ -176,7 +205,7 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 namespace nfft {
 
 template <int LOG_TILE, int LOAD, int STORE>
-static void emu_pass(const PassArgs& a, long long ntiles) {
+static void emu_pass(const PassArgs& a, long long t0, long long t1) {
     using T = real_t;
     using V = C2<T>;
     constexpr int THREADS = (1 << LOG_TILE) / 16;
@@ -216,7 +245,7 @@ static void emu_pass(const PassArgs& a, long long ntiles) {
             lns += lr;
         }
     };
-    for (long long tile = 0; tile < ntiles; ++tile) {
+    for (long long tile = t0; tile < t1; ++tile) {
         const long long line0 = tile << a.logJ;
         if (line0 >= a.nlines) continue;
         for (auto& x : sm) x = mkc((T)NAN, (T)NAN);
@@ -241,7 +270,7 @@ static void emu_pass(const PassArgs& a, long long ntiles) {
     }
 }
 
-using EmuFn = void (*)(const PassArgs&, long long);
+using EmuFn = void (*)(const PassArgs&, long long, long long);
 
 #define NFFT_PAIRS(X) \
     X(LD_C, ST_C) X(LD_C, ST_R) X(LD_C, ST_T2) X(LD_C, ST_T3) X(LD_C, ST_T4) X(LD_C, ST_BLUE) X(LD_T2, ST_C) \
@@ -265,7 +294,7 @@ bool launch_pass(const PassArgs& a, int ld, int st, int log_tile, long long ntil
         return false;
     }
     g_launches++;
-    f(a, ntiles);
+    f(a, 0, ntiles);
     return true;
 }
 
@@ -328,7 +357,7 @@ bool set_kernel_attributes() { return true; }
 // ---- specialized (lean) pass kernels: the kernel body of nfft_lean.cuh, with
 // every phase run for all threads before the next (its __syncthreads points)
 template <int LOGR, int LOGT, bool CI, bool CO, int LD, int ST>
-static void emu_lean(const PassArgs& a, long long ntiles) {
+static void emu_lean(const PassArgs& a, long long t0, long long t1) {
     using T = real_t;
     using V = C2<T>;
     using Lt = Lean<T, LOGR, LOGT, CI, CO, LD, ST>;
@@ -351,7 +380,7 @@ static void emu_lean(const PassArgs& a, long long ntiles) {
                 Lt::template write_smem<S>(sm.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
             }
     };
-    for (long long tile = 0; tile < ntiles; ++tile) {
+    for (long long tile = t0; tile < t1; ++tile) {
         const long long line0 = tile << Lt::LOGJ;
         if (line0 >= a.nlines) continue;
         for (auto& x : sm) x = mkc((T)NAN, (T)NAN);
@@ -648,7 +677,7 @@ bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStrea
     return true;
 }
 
-using EmuLean = void (*)(const PassArgs&, long long);
+using EmuLean = void (*)(const PassArgs&, long long, long long);
 static std::map<unsigned, EmuLean>& emu_lean_table() {
     static std::map<unsigned, EmuLean> t = [] {
         std::map<unsigned, EmuLean> m;
@@ -671,10 +700,85 @@ bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, lo
     }
     g_launches++;
     g_lean_launches++;
-    it->second(a, ntiles);
+    it->second(a, 0, ntiles);
     return true;
 }
 long long launch_count() { return g_launches; }
+
+bool launch_post(cplx_t* post, long long n, cudaStream_t) {
+    for (long long q = 0; q < n; ++q) {
+        long double ang = 3.141592653589793238462643383279502884L * (long double)q / (long double)(2 * n);
+        post[q] = mkc((real_t)cosl(ang), (real_t)-sinl(ang));
+    }
+    return true;
+}
+
+// ---- the persistent queue: items run in claim order by one virtual CTA.  In
+// that order every dependency of an item has been published before the item
+// is claimed, so a counter short of its target is a dependency that can never
+// be published; the device kernel's bounded wait gives up on it, and so does
+// this emulation (abort flag + status word).
+int queue_grid(const DeviceCtx*) { return 296; }
+static long long g_queue_items = 0;
+bool launch_queue(const QueueArgs& q, int, cudaStream_t) {
+    using T = real_t;
+    static std::map<int, EmuLean> table = [] {
+        std::map<int, EmuLean> m;
+#define X(R, CI, CO, LD, ST) m[qop_lean(R, CI, CO, LD, ST)] = emu_lean<R, QUEUE_LOGT, CI != 0, CO != 0, LD, ST>;
+        NFFT_QUEUE_LEAN(X)
+#undef X
+#define X(LD, ST) m[qop_gen(LD, ST)] = emu_pass<QUEUE_LOG_TILE, LD, ST>;
+        NFFT_QUEUE_GENERIC(X)
+#undef X
+        return m;
+    }();
+    g_launches++;
+    unsigned* ctr = q.ctr;
+    for (long long i = 0; i < q.nitems; ++i) {
+        const QItem it = q.items[i];
+        QDesc d = q.descs[it.desc];
+        if (d.flags & QD_IN_USER) d.a.in = (const char*)q.user_in + (size_t)d.a.in;
+        if (d.flags & QD_OUT_USER) d.a.out = (char*)q.user_out + (size_t)d.a.out;
+        if (it.wait >= 0 && ctr[it.wait] < (unsigned)it.target) {
+            ctr[QCTR_ABORT] = 1;
+            if (!*q.status) *q.status = (int)(i + 1);
+            return true;
+        }
+        ++g_queue_items;
+        const long long t0 = it.tile0, t1 = it.tile0 + it.ntiles;
+        const TwTables<T>* tw = (const TwTables<T>*)d.a.tw;
+        if (it.op == qop_unpack(ST_R) || it.op == qop_unpack(ST_T2)) {
+            for (long long t = t0; t < t1; ++t) {
+                long long w0, w1;
+                unpack_tile_range(d.a, t, w0, w1);
+                for (long long w = w0; w < w1; ++w) {
+                    if (it.op == qop_unpack(ST_R)) unpack_item<T, ST_R>(d.a, tw, (const C2<T>*)d.z, d.zdist, w);
+                    else unpack_item<T, ST_T2>(d.a, tw, (const C2<T>*)d.z, d.zdist, w);
+                }
+            }
+        } else if (it.op == QOP_SCALAR) {
+            const PassArgs& a = d.a;
+            for (long long t = t0; t < t1; ++t)
+                for (long long j = t * SCALAR_TILE; j < std::min<long long>((t + 1) * SCALAR_TILE, a.nlines); ++j) {
+                    const T* x = (const T*)a.in + NFFT_GLD(&a.in_tab[j]);
+                    T* y = (T*)a.out + NFFT_GLD(&a.out_tab[j]);
+                    const T re = (T)(a.scale * (double)NFFT_GLD(&x[0]));
+                    const T im = (a.conj_in && a.dst) ? (T)(a.scale * (double)NFFT_GLD(&x[1])) : (T)0;
+                    NFFT_GST(&y[0], re);
+                    if (a.conj_out) NFFT_GST(&y[1], im);
+                }
+        } else {
+            auto f = table.find(it.op);
+            if (f == table.end()) {
+                fprintf(stderr, "nfft_emu: queue item %lld has unknown branch 0x%x\n", i, it.op);
+                abort();
+            }
+            f->second(d.a, t0, t1);
+        }
+        if (it.done >= 0) ctr[it.done] += (unsigned)it.ntiles;
+    }
+    return true;
+}
 
 }  // namespace nfft
 
@@ -697,4 +801,5 @@ long long nfft_emu_launches(void) { return nfft::g_launches; }
 long long nfft_emu_lean_launches(void) { return nfft::g_lean_launches; }
 long long nfft_emu_cluster_launches(void) { return nfft::g_cluster_launches; }
 long long nfft_emu_checks(void) { return emu::n_checks; }
+long long nfft_emu_queue_items(void) { return nfft::g_queue_items; }
 }
