@@ -127,6 +127,9 @@ struct notorious_fft_plan {
     // temporary of the multi-dimensional inverse real transform
     void* nd_tmp = nullptr;
     size_t nd_tmp_bytes = 0;
+    // counters of the resident two-pass kernel
+    unsigned* res_ctr = nullptr;
+    size_t res_ctr_n = 0;
     std::mutex mu;
 };
 
@@ -208,6 +211,19 @@ bool set_kernel_attributes();
 struct QueueArgs;
 int queue_grid(const DeviceCtx* c);   // resident CTAs (0 on error)
 bool launch_queue(const QueueArgs& q, int grid, cudaStream_t s);
+
+// Resident two-pass kernels (nfft_resident.cu): both Stockham passes of a
+// batched power-of-two complex DFT in one persistent launch, the inter-pass
+// scratch kept in L2.  ctr: B + 3 counters of device memory.
+struct ResidentEntry {
+    int r1, r2, logt;
+    const void* fn;
+    size_t smem;
+};
+const ResidentEntry* resident_find(int r1, int r2);
+bool resident_set_attributes();
+bool launch_resident(const DeviceCtx* c, const PassArgs& a1, const PassArgs& a2, int r1, int r2, long long B,
+                     unsigned* ctr, cudaStream_t s);
 
 // Ragged batches (nfft_queue_build.cu).  Offsets in reals, NULL: packed.
 notorious_fft_batch* batch_create_default(int count, const int* kinds, const int* Ns, const long long* in_off,

@@ -36,6 +36,7 @@ enum LoadOp : int {
     LD_R2C = 6,   // realdft: N reals read pairwise as N/2 complex (any alignment / stride)
     LD_BLUE_R = 7,   // Bluestein of N reals (realdft of any N): (x_p, 0) times the chirp
     LD_BLUE_T2 = 8,  // Bluestein DCT-2 of any N: even / reversed-odd reorder of N reals, times the chirp
+    LD_FILT = 9,     // Bluestein: conj(spectrum * filter), the input of the inverse M-point FFT
 };
 // Fused output operators.
 enum StoreOp : int {
@@ -49,7 +50,7 @@ enum StoreOp : int {
     ST_BLUE_R = 7,   // Bluestein realdft of any N: bins 0 .. N/2 of the windowed, chirped output
     ST_BLUE_T2 = 8,  // Bluestein DCT-2 of any N: y_q = 2 Re(e^{-i pi q/2N} V_q), q < N
 };
-constexpr int NUM_LOAD_OPS = 9, NUM_STORE_OPS = 9;
+constexpr int NUM_LOAD_OPS = 10, NUM_STORE_OPS = 9;
 
 constexpr int MAX_LINE_DIMS = 4;
 constexpr int MAX_SUB = 4;
@@ -115,6 +116,9 @@ NFFT_HD C2<T> load_elem(const PassArgs& a, const TwTables<T>* tw, long long base
         if constexpr (OP == LD_BLUE_R) r = NFFT_GLD(&x[p * es]);
         else r = (p < (a.N + 1) / 2) ? NFFT_GLD(&x[(2 * p) * es]) : NFFT_GLD(&x[(2 * a.N - 1 - 2 * p) * es]);
         return cscale(NFFT_GLD(&((const V*)a.chirp)[p]), r);
+    } else if constexpr (OP == LD_FILT) {
+        const V v = NFFT_GLD(&((const V*)a.in)[base + p * a.in_estride]);
+        return cconj(cmul(v, NFFT_GLD(&((const V*)a.filt)[p])));
     } else if constexpr (OP == LD_R2C) {
         const T* x = (const T*)a.in + base;
         const long long es = a.in_estride;

@@ -285,6 +285,17 @@ static void set_lines(PassArgs& a, const View& src, const View& dst, long long n
     a.nlines = n;
 }
 
+// NOTORIOUS_FFT_RESIDENT=0 runs two-pass transforms as two launches per chunk
+// instead of one resident launch.
+static bool resident_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NOTORIOUS_FFT_RESIDENT");
+        v = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    return v == 1;
+}
+
 // L2 policy: NOTORIOUS_FFT_CACHE_HINTS=0 turns the hints off.
 static bool cache_hints() {
     static int v = -1;
@@ -311,11 +322,11 @@ static int tw_mode() {
     return v;
 }
 
+// Arguments of one pass (everything but the tile shape and the kernel).
 // in_scratch / out_scratch: the pass reads / writes an inter-pass scratch buffer.
-bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR, int tile,
-              int nsub, const int* sub, const OpSpec& op, bool first, bool last, int mid, int logNs_out,
-              const cplx_t* chirp, const cplx_t* filt, cudaStream_t s, bool in_scratch, bool out_scratch) {
-    PassArgs a;
+static void make_pass_args(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR,
+                           int nsub, const int* sub, const OpSpec& op, bool first, bool last, int mid, int logNs_out,
+                           const cplx_t* chirp, const cplx_t* filt, bool in_scratch, bool out_scratch, PassArgs& a) {
     fill_common(a, c);
     a.tw_mode = tw_mode();
     if (cache_hints() && (in_scratch || out_scratch)) {
@@ -350,6 +361,15 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
     a.filt = filt;
     a.mid = mid;
     a.vjp = op.vjp;
+    a.post = op.post;
+}
+
+bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, int logNs, int logR, int tile,
+              int nsub, const int* sub, const OpSpec& op, bool first, bool last, int mid, int logNs_out,
+              const cplx_t* chirp, const cplx_t* filt, cudaStream_t s, bool in_scratch, bool out_scratch) {
+    PassArgs a;
+    make_pass_args(c, src, dst, logL, logNs, logR, nsub, sub, op, first, last, mid, logNs_out, chirp, filt, in_scratch,
+                   out_scratch, a);
     int ldop = first ? op.ld : LD_C;
     int stop = last ? op.st : ST_C;
     int logE_max = tile;
@@ -361,7 +381,6 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
         set_error(6, "pass radix 2^%d exceeds tile 2^%d", logR, tile);
         return false;
     }
-    a.post = op.post;
     if (Recorder* rec = recorder()) {
         // queue form: a branch of the persistent 256-thread kernel.  Scratch
         // written earlier in the same launch is read through L2 (hint 3).
@@ -488,6 +507,13 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
     if (chunk > outer) chunk = outer;
     const bool paired_epilogue = op.paired;
     const int nbuf = paired_epilogue ? (np >= 2 ? 2 : 1) : (np >= 3 ? 2 : 1);
+    // one resident launch per chunk for plain two-pass complex transforms of
+    // contiguous lines
+    const ResidentEntry* res = nullptr;
+    if (np == 2 && !strided && !paired_epilogue && op.ld == LD_C && op.st == ST_C && !op.tc && !recorder() &&
+        src.nb <= 1 && dst.nb <= 1 && resident_enabled() && !lean_disabled())
+        res = resident_find(sch.plog[0], sch.plog[1]);
+    const bool use_resident = res != nullptr;
     void* buf[2] = {nullptr, nullptr};
     for (int i = 0; i < nbuf; ++i) {
         buf[i] = get_scratch(p, i, (size_t)chunk * per_outer);
@@ -502,6 +528,35 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
             vd.ptr = (char*)dst.ptr + (size_t)(o0 * dst.str[dst.nb - 1]) *
                                           ((op.st == ST_C || op.st == ST_R || op.st == ST_BLUE) ? sizeof(cplx_t) : sizeof(real_t));
             vd.cnt[dst.nb - 1] = cn;
+        }
+        if (use_resident) {
+            // both passes in one persistent launch, the scratch kept in L2
+            View sv = scratch_view(buf[0], vs, L, false);
+            PassArgs a1, a2;
+            make_pass_args(c, vs, sv, logL, 0, sch.plog[0], sch.nsub[0], sch.sub[0], op, true, false, 0, 0, nullptr,
+                           nullptr, false, true, a1);
+            make_pass_args(c, sv, vd, logL, sch.plog[0], sch.plog[1], sch.nsub[1], sch.sub[1], op, false, true, 0,
+                           sch.plog[0], nullptr, nullptr, true, false, a2);
+            const int lt = res->logt;
+            a1.logJ = lt + 4 - sch.plog[0];
+            a2.logJ = lt + 4 - sch.plog[1];
+            a1.hint_in = 1;
+            a1.hint_out = 2;
+            a2.hint_in = 3;
+            a2.discard_in = 1;
+            a2.hint_out = 1;
+            const long long B = vs.lines();
+            if (p->res_ctr_n < (size_t)(B + 3)) {
+                if (p->res_ctr) cudaFree(p->res_ctr);
+                p->res_ctr = nullptr;
+                p->res_ctr_n = 0;
+                if (!cuda_ok(cudaMalloc((void**)&p->res_ctr, sizeof(unsigned) * (size_t)(B + 3)),
+                             "cudaMalloc(resident counters)"))
+                    return false;
+                p->res_ctr_n = (size_t)(B + 3);
+            }
+            if (!launch_resident(c, a1, a2, sch.plog[0], sch.plog[1], B, p->res_ctr, s)) return false;
+            continue;
         }
         View cur = vs;
         int logNs = 0;
@@ -618,8 +673,28 @@ static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const 
             cur = out;
             bi ^= 1;
         }
-        // last forward pass + filter + first inverse pass
-        {
+        if (recorder()) {
+            // queue form: the last forward pass and the first inverse pass stay
+            // separate specialized passes; the filter product and conjugation
+            // are the inverse pass's load operator (one more sweep of M, no
+            // generic middle pass)
+            View out = scratch_view(buf[bi], vs, M, false);
+            if (!run_pass(c, cur, out, logM, logNs, f.plog[np - 1], f.tile[np - 1], f.nsub[np - 1], f.sub[np - 1], op,
+                          false, false, 0, logNs, ax.chirp, ax.filt, s))
+                return false;
+            cur = out;
+            bi ^= 1;
+            View out2 = scratch_view(buf[bi], vs, M, false);
+            OpSpec o = op;
+            o.ld = LD_FILT;
+            o.conj_in = 0;
+            if (!run_pass(c, cur, out2, logM, 0, g.plog[0], g.tile[0], g.nsub[0], g.sub[0], o, true, false, 0, 0,
+                          ax.chirp, ax.filt, s))
+                return false;
+            cur = out2;
+            bi ^= 1;
+        } else {
+            // last forward pass + filter + first inverse pass
             View out = scratch_view(buf[bi], vs, M, false);
             OpSpec o = op;
             if (!run_pass(c, cur, out, logM, logNs, f.plog[np - 1], f.tile[np - 1], f.nsub[np - 1], f.sub[np - 1], o,
@@ -751,6 +826,7 @@ void plan_destroy(notorious_fft_plan* p) {
     if (p->s_h2d) cudaStreamDestroy(p->s_h2d);
     if (p->s_d2h) cudaStreamDestroy(p->s_d2h);
     if (p->nd_tmp) cudaFree(p->nd_tmp);
+    if (p->res_ctr) cudaFree(p->res_ctr);
     if (p->stage_out) cudaFree(p->stage_out);
     if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
     delete p;

@@ -57,7 +57,7 @@ constexpr int QUEUE_LOGT = 8;
 constexpr int QUEUE_THREADS = 1 << QUEUE_LOGT;
 constexpr int QUEUE_LOG_TILE = 12;
 
-// Specialized (lean) branches: X(LOGR, COL_IN, COL_OUT, LOAD, STORE), in three
+// Specialized (lean) branches: X(LOGR, COL_IN, COL_OUT, LOAD, STORE), in four
 // families (each compiled in its own translation unit, nfft_queue_b*.cu).
 // Complex passes: single-pass rows, first (column in / row out) passes.
 #define NFFT_QUEUE_LEAN_A(X)                                                                        \
@@ -82,7 +82,24 @@ constexpr int QUEUE_LOG_TILE = 12;
     X(4, 0, 0, LD_T2, ST_T2) X(5, 0, 0, LD_T2, ST_T2) X(6, 0, 0, LD_T2, ST_T2)                      \
     X(7, 0, 0, LD_T2, ST_T2) X(8, 0, 0, LD_T2, ST_T2) X(9, 0, 0, LD_T2, ST_T2)                      \
     X(10, 0, 0, LD_T2, ST_T2) X(11, 0, 0, LD_T2, ST_T2) X(12, 0, 0, LD_T2, ST_T2)
-#define NFFT_QUEUE_LEAN(X) NFFT_QUEUE_LEAN_A(X) NFFT_QUEUE_LEAN_B(X) NFFT_QUEUE_LEAN_C(X)
+// Multi-pass Bluestein: chirp-premultiplied first forward passes, the filter
+// product fused into the first inverse pass, window + chirp in the last one.
+#define NFFT_QUEUE_LEAN_D(X)                                                                        \
+    X(6, 1, 0, LD_BLUE, ST_C) X(7, 1, 0, LD_BLUE, ST_C) X(8, 1, 0, LD_BLUE, ST_C)                   \
+    X(9, 1, 0, LD_BLUE, ST_C) X(10, 1, 0, LD_BLUE, ST_C)                                            \
+    X(6, 1, 0, LD_BLUE_R, ST_C) X(7, 1, 0, LD_BLUE_R, ST_C) X(8, 1, 0, LD_BLUE_R, ST_C)             \
+    X(9, 1, 0, LD_BLUE_R, ST_C) X(10, 1, 0, LD_BLUE_R, ST_C)                                        \
+    X(6, 1, 0, LD_BLUE_T2, ST_C) X(7, 1, 0, LD_BLUE_T2, ST_C) X(8, 1, 0, LD_BLUE_T2, ST_C)          \
+    X(9, 1, 0, LD_BLUE_T2, ST_C) X(10, 1, 0, LD_BLUE_T2, ST_C)                                      \
+    X(5, 1, 0, LD_FILT, ST_C) X(6, 1, 0, LD_FILT, ST_C) X(7, 1, 0, LD_FILT, ST_C)                   \
+    X(8, 1, 0, LD_FILT, ST_C) X(9, 1, 0, LD_FILT, ST_C) X(10, 1, 0, LD_FILT, ST_C)                  \
+    X(6, 1, 1, LD_C, ST_BLUE) X(7, 1, 1, LD_C, ST_BLUE) X(8, 1, 1, LD_C, ST_BLUE)                   \
+    X(9, 1, 1, LD_C, ST_BLUE) X(10, 1, 1, LD_C, ST_BLUE)                                            \
+    X(6, 1, 1, LD_C, ST_BLUE_R) X(7, 1, 1, LD_C, ST_BLUE_R) X(8, 1, 1, LD_C, ST_BLUE_R)             \
+    X(9, 1, 1, LD_C, ST_BLUE_R) X(10, 1, 1, LD_C, ST_BLUE_R)                                        \
+    X(6, 1, 1, LD_C, ST_BLUE_T2) X(7, 1, 1, LD_C, ST_BLUE_T2) X(8, 1, 1, LD_C, ST_BLUE_T2)          \
+    X(9, 1, 1, LD_C, ST_BLUE_T2) X(10, 1, 1, LD_C, ST_BLUE_T2)
+#define NFFT_QUEUE_LEAN(X) NFFT_QUEUE_LEAN_A(X) NFFT_QUEUE_LEAN_B(X) NFFT_QUEUE_LEAN_C(X) NFFT_QUEUE_LEAN_D(X)
 
 // Generic branches (4096-point tile, any pass radix): X(LOAD, STORE).
 #define NFFT_QUEUE_GENERIC(X)                                                                       \
@@ -90,7 +107,7 @@ constexpr int QUEUE_LOG_TILE = 12;
     X(LD_T3, ST_C) X(LD_T3, ST_T3) X(LD_IR, ST_C) X(LD_T4, ST_C) X(LD_T4, ST_T4) X(LD_BLUE, ST_C)   \
     X(LD_BLUE, ST_BLUE) X(LD_R2C, ST_C) X(LD_R2C, ST_R) X(LD_C, ST_C2R) X(LD_IR, ST_C2R)            \
     X(LD_BLUE_R, ST_C) X(LD_BLUE_R, ST_BLUE_R) X(LD_C, ST_BLUE_R) X(LD_BLUE_T2, ST_C)               \
-    X(LD_BLUE_T2, ST_BLUE_T2) X(LD_C, ST_BLUE_T2)
+    X(LD_BLUE_T2, ST_BLUE_T2) X(LD_C, ST_BLUE_T2) X(LD_FILT, ST_C)
 
 // Branch keys.
 constexpr int QOP_LEAN_BASE = 0x100000, QOP_GEN_BASE = 0x200000, QOP_UNPACK_BASE = 0x300000;

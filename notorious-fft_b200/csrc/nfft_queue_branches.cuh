@@ -2,7 +2,7 @@
 // (nfft_queue_kernel.cu).  Each branch runs all tiles of one queue item with
 // the same tile bodies as the standalone pass kernels.  The branches are
 // separate, non-inlined device functions, instantiated in the translation
-// units nfft_queue_b0..b3.cu (compiled in parallel as relocatable device code
+// units nfft_queue_b0..b4.cu (compiled in parallel as relocatable device code
 // with the kernel's register budget) and reached through the kernel's
 // dispatcher by the device linker.
 #pragma once

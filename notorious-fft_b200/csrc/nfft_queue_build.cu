@@ -89,8 +89,8 @@ struct BucketPlan {
 // Build options (defaults from the environment, see batch_default_options).
 struct BatchOptions {
     int use_tuned = 1;           // take pass splits from the tune cache
-    int tiles_multi = 1;         // tiles per item of multi-pass transforms
-    int tiles_single = 4;        // tiles per item of single-pass transforms
+    int tiles_multi = 4;         // tiles per item of multi-pass transforms
+    int tiles_single = 8;        // tiles per item of single-pass transforms
     long long group_bytes = 4ll << 20;
     long long lag = -1;          // items between dependent passes (-1: 3 x resident CTAs)
     long long spin_limit = 1ll << 22;
@@ -99,8 +99,8 @@ struct BatchOptions {
 
 BatchOptions batch_default_options() {
     BatchOptions o;
-    o.tiles_multi = (int)std::max(1ll, env_ll("NOTORIOUS_FFT_QUEUE_TILES_MULTI", 1));
-    o.tiles_single = (int)std::max(1ll, env_ll("NOTORIOUS_FFT_QUEUE_TILES_SINGLE", 4));
+    o.tiles_multi = (int)std::max(1ll, env_ll("NOTORIOUS_FFT_QUEUE_TILES_MULTI", 4));
+    o.tiles_single = (int)std::max(1ll, env_ll("NOTORIOUS_FFT_QUEUE_TILES_SINGLE", 8));
     o.group_bytes = std::max(1ll, env_ll("NOTORIOUS_FFT_QUEUE_GROUP_KB", 4096)) << 10;
     o.lag = env_ll("NOTORIOUS_FFT_QUEUE_LAG", -1);
     o.spin_limit = std::max(1ll, env_ll("NOTORIOUS_FFT_QUEUE_SPIN", 1ll << 22));

@@ -67,7 +67,7 @@ __device__ __noinline__ int queue_wait(const QueueArgs& q, int wait, unsigned ta
 }
 
 // Branch functions (nfft_queue_branches.cuh), compiled in the translation
-// units nfft_queue_b0..b3.cu and linked as relocatable device code.
+// units nfft_queue_b0..b4.cu and linked as relocatable device code.
 template <typename T, int R, int CI, int CO, int LD, int ST>
 __device__ void qb_lean(const QDesc* d, long long tile0, int ntiles, unsigned char* smraw);
 template <typename T, int LD, int ST>
@@ -162,7 +162,6 @@ int queue_grid(const DeviceCtx* c) {
 
 bool launch_queue(const QueueArgs& q, int grid, cudaStream_t s) {
     queue_kernel<real_t><<<grid, QUEUE_THREADS, QUEUE_SMEM, s>>>(q);
-    note_launch();
     return cuda_ok(cudaGetLastError(), "queue kernel launch");
 }
 

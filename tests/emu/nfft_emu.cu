@@ -198,6 +198,8 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 #include "../../notorious-fft_b200/csrc/nfft_cluster.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_tc.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_queue.h"
+#include "../../notorious-fft_b200/csrc/nfft_resident.cuh"
+#include "../../notorious-fft_b200/csrc/nfft_resident_list.h"
 
 // ---------------------------------------------------------------------------
 // emulated launches: the kernels' phase functions for every thread
@@ -705,6 +707,69 @@ bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, lo
 }
 long long launch_count() { return g_launches; }
 
+// ---- resident two-pass kernels: the decoded work order run by one virtual
+// CTA (a short lag so the interleaved region of the order is exercised); a
+// pass-2 tile whose transform's pass-1 tiles are not all done aborts.
+static std::vector<ResidentEntry>& emu_resident_registry() {
+    static std::vector<ResidentEntry> v = [] {
+        std::vector<ResidentEntry> r;
+#define X(R1, R2, LT) r.push_back(ResidentEntry{R1, R2, LT, nullptr, 0});
+        NFFT_RESIDENT_A(X) NFFT_RESIDENT_B(X)
+#undef X
+        return r;
+    }();
+    return v;
+}
+const ResidentEntry* resident_find(int r1, int r2) {
+    for (auto& e : emu_resident_registry())
+        if (e.r1 == r1 && e.r2 == r2) return &e;
+    return nullptr;
+}
+bool resident_set_attributes() { return true; }
+static long long g_resident_launches = 0;
+bool launch_resident(const DeviceCtx*, const PassArgs& a1, const PassArgs& a2, int r1, int r2, long long B,
+                     unsigned*, cudaStream_t) {
+    static std::map<std::pair<int, int>, std::pair<EmuLean, EmuLean>> fns = [] {
+        std::map<std::pair<int, int>, std::pair<EmuLean, EmuLean>> m;
+#define X(R1, R2, LT) \
+    m[{R1, R2}] = {emu_lean<R1, LT, true, false, LD_C, ST_C>, emu_lean<R2, LT, true, true, LD_C, ST_C>};
+        NFFT_RESIDENT_A(X) NFFT_RESIDENT_B(X)
+#undef X
+        return m;
+    }();
+    const ResidentEntry* e = resident_find(r1, r2);
+    if (!e) {
+        set_error(6, "no resident kernel for radices 2^%d x 2^%d", r1, r2);
+        return false;
+    }
+    const auto& f = fns[{r1, r2}];
+    const int lt = r1 + r2 - (e->logt + 4);
+    const long long T = 1ll << lt, lag = std::min<long long>(B, 2);
+    std::vector<long long> done((size_t)B, 0);
+    g_launches++;
+    g_resident_launches++;
+    for (long long g = 0; g < 2 * B * T; ++g) {
+        int pass;
+        long long tr, tile;
+        resident_decode(g, B, lag, lt, pass, tr, tile);
+        if (tr < 0 || tr >= B || tile < 0 || tile >= T) {
+            fprintf(stderr, "nfft_emu: resident item %lld decodes outside the launch\n", g);
+            abort();
+        }
+        if (pass == 2) {
+            if (done[tr] != T) {
+                fprintf(stderr, "nfft_emu: resident pass-2 item %lld before its pass 1\n", g);
+                abort();
+            }
+            f.second(a2, (tr << lt) + tile, (tr << lt) + tile + 1);
+        } else {
+            f.first(a1, (tr << lt) + tile, (tr << lt) + tile + 1);
+            done[tr]++;
+        }
+    }
+    return true;
+}
+
 bool launch_post(cplx_t* post, long long n, cudaStream_t) {
     for (long long q = 0; q < n; ++q) {
         long double ang = 3.141592653589793238462643383279502884L * (long double)q / (long double)(2 * n);
@@ -802,4 +867,5 @@ long long nfft_emu_lean_launches(void) { return nfft::g_lean_launches; }
 long long nfft_emu_cluster_launches(void) { return nfft::g_cluster_launches; }
 long long nfft_emu_checks(void) { return emu::n_checks; }
 long long nfft_emu_queue_items(void) { return nfft::g_queue_items; }
+long long nfft_emu_resident_launches(void) { return nfft::g_resident_launches; }
 }

@@ -190,10 +190,12 @@ def test_queue_structure(emu_d):
     """Items of a multi-pass bucket: one group per transform at a 1 KB group
     target, two dependent stages each; every item runs in the emulated launch."""
     os.environ["NOTORIOUS_FFT_QUEUE_GROUP_KB"] = "1"
+    os.environ["NOTORIOUS_FFT_QUEUE_TILES_MULTI"] = "1"
     try:
         b = emu_d.mkbatch(["dft"] * 3, [8192] * 3)
     finally:
         del os.environ["NOTORIOUS_FFT_QUEUE_GROUP_KB"]
+        del os.environ["NOTORIOUS_FFT_QUEUE_TILES_MULTI"]
     info = b.info()
     # 8192 points = 2 tiles of 4096 per pass, two passes, one tile per item
     assert info["tiles"] == 3 * 2 * 2 and info["items"] == 12
