@@ -217,8 +217,10 @@ bool launch_queue(const QueueArgs& q, int grid, cudaStream_t s);
 // scratch kept in L2.  ctr: B + 3 counters of device memory.
 struct ResidentEntry {
     int r1, r2, logt;
-    const void* fn;
+    const void* fn;         // plain resident kernel
     size_t smem;
+    const void* fn_pf;      // software-pipelined variant (cp.async staging)
+    size_t smem_pf;
 };
 const ResidentEntry* resident_find(int r1, int r2);
 bool resident_set_attributes();

@@ -124,8 +124,14 @@ struct Lean {
             for (int m = 0; m < 16; ++m)
                 v[m] = load_elem<T, LOAD>(a, tw, ln.bin, ln.j + ((long long)(i + (m << (LOGR - 4))) << a.logNj));
         }
+        pre_twiddle_dft(a, tw, ln.j, i, v);
+    }
+
+    // Pass pre-twiddle W_{Ns R}^{r k} (k = j mod Ns) of the 16 points r = i + m R/16
+    // of line j held by this thread, then the first radix-16 DFT.
+    static NFFT_HD void pre_twiddle_dft(const PassArgs& a, const TwTables<T>* tw, long long j, int i, C2<T>* v) {
         if (a.logNs > 0) {
-            const long long k = ln.j & ((1ll << a.logNs) - 1);
+            const long long k = j & ((1ll << a.logNs) - 1);
             if (k) {
                 // W_{Ns R}^{(i + m R/16) k} = W_{Ns R}^{i k} * (W_{16 Ns}^{k})^m
                 if (a.tw_mode == 2) {

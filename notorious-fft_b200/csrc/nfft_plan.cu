@@ -285,15 +285,20 @@ static void set_lines(PassArgs& a, const View& src, const View& dst, long long n
     a.nlines = n;
 }
 
-// NOTORIOUS_FFT_RESIDENT=0 runs two-pass transforms as two launches per chunk
-// instead of one resident launch.
-static bool resident_enabled() {
-    static int v = -1;
-    if (v < 0) {
+// Two-pass complex transforms of 2^logL points: one resident launch per chunk
+// (both passes, scratch in L2) or two launches.  The resident form halves the
+// DRAM traffic but is bound by the SMs' tile throughput, which the two
+// launches already nearly saturate at ~90% of HBM bandwidth; on B200 it wins
+// only for FP64 at 2^19 points.  NOTORIOUS_FFT_RESIDENT=1 / 0 forces it on /
+// off for every size.
+static bool resident_enabled(int logL) {
+    static int v = -2;
+    if (v == -2) {
         const char* e = getenv("NOTORIOUS_FFT_RESIDENT");
-        v = (e && atoi(e) == 0) ? 0 : 1;
+        v = e ? (atoi(e) != 0 ? 1 : 0) : -1;
     }
-    return v == 1;
+    if (v >= 0) return v == 1;
+    return sizeof(real_t) == 8 && logL == 19;
 }
 
 // L2 policy: NOTORIOUS_FFT_CACHE_HINTS=0 turns the hints off.
@@ -511,7 +516,7 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
     // contiguous lines
     const ResidentEntry* res = nullptr;
     if (np == 2 && !strided && !paired_epilogue && op.ld == LD_C && op.st == ST_C && !op.tc && !recorder() &&
-        src.nb <= 1 && dst.nb <= 1 && resident_enabled() && !lean_disabled())
+        src.nb <= 1 && dst.nb <= 1 && resident_enabled(logL) && !lean_disabled())
         res = resident_find(sch.plog[0], sch.plog[1]);
     const bool use_resident = res != nullptr;
     void* buf[2] = {nullptr, nullptr};

@@ -31,16 +31,29 @@ const ResidentEntry* resident_find(int r1, int r2) {
 bool resident_set_attributes() {
     for (auto& e : resident_registry())
         if (!cuda_ok(cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem),
+                     "cudaFuncSetAttribute(resident kernel)") ||
+            !cuda_ok(cudaFuncSetAttribute(e.fn_pf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem_pf),
                      "cudaFuncSetAttribute(resident kernel)"))
             return false;
     return true;
 }
 
-// Persistent CTAs of one entry on this device.
-static int resident_grid(const ResidentEntry& e, const DeviceCtx* c) {
+// NOTORIOUS_FFT_RESIDENT_PREFETCH=1 selects the software-pipelined resident
+// kernels (tile k+1 staged by cp.async while tile k computes).  Off by
+// default: its staging buffer costs one CTA per SM, and on B200 that loses
+// more than the hidden load latency gains.
+static bool prefetch_enabled() {
+    static const int v = [] {
+        const char* e = getenv("NOTORIOUS_FFT_RESIDENT_PREFETCH");
+        return (e && atoi(e) != 0) ? 1 : 0;
+    }();
+    return v == 1;
+}
+
+// Persistent CTAs of one kernel on this device.
+static int resident_grid(const void* fn, int threads, size_t smem, const DeviceCtx* c) {
     int per_sm = 0;
-    if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, e.fn, 1 << e.logt, e.smem),
-                 "resident kernel occupancy"))
+    if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem), "resident kernel occupancy"))
         return 0;
     return std::max(1, per_sm) * c->sm_count;
 }
@@ -52,7 +65,10 @@ bool launch_resident(const DeviceCtx* c, const PassArgs& a1, const PassArgs& a2,
         set_error(6, "no resident kernel for radices 2^%d x 2^%d", r1, r2);
         return false;
     }
-    const int grid = resident_grid(*e, c);
+    const bool pf = prefetch_enabled();
+    const void* fn = pf ? e->fn_pf : e->fn;
+    const size_t smem = pf ? e->smem_pf : e->smem;
+    const int grid = resident_grid(fn, 1 << e->logt, smem, c);
     if (grid <= 0) return false;
     ResidentArgs r;
     r.B = B;
@@ -84,7 +100,7 @@ bool launch_resident(const DeviceCtx* c, const PassArgs& a1, const PassArgs& a2,
     if (!cuda_ok(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * (size_t)(B + 3), s), "resident counter reset")) return false;
     void* args[3] = {(void*)&a1, (void*)&a2, (void*)&r};
     note_launch();
-    return cuda_ok(cudaLaunchKernel(e->fn, dim3(grid), dim3(1 << e->logt), args, e->smem, s), "resident kernel launch");
+    return cuda_ok(cudaLaunchKernel(fn, dim3(grid), dim3(1 << e->logt), args, smem, s), "resident kernel launch");
 }
 
 }  // namespace nfft

@@ -66,6 +66,23 @@ NFFT_HD void resident_decode(long long g, long long B, long long lag, int lt, in
     tile = g & (T - 1);
 }
 
+// Line of thread t in global tile g of a resident pass with radix 2^logR and
+// 2^logJ lines per tile (column mapping; the lines of a transform are its
+// 2^logNj Stockham lines, the batch dim outermost): the line's offsets and
+// Stockham index, and the thread's butterfly index i.  Equivalent to
+// line_setup for these passes, with shifts instead of divisions.
+NFFT_HD void resident_line(const PassArgs& a, int logJ, int logR, long long g, int t, long long& bin, long long& bout,
+                           long long& j, int& i) {
+    const int l = t & ((1 << logJ) - 1);
+    i = t >> logJ;
+    (void)logR;
+    const long long lam = (g << logJ) + l;
+    const long long b = lam >> a.logNj;
+    j = lam & ((1ll << a.logNj) - 1);
+    bin = a.ndims > 1 ? b * a.istr[1] : 0;
+    bout = a.ndims > 1 ? b * a.ostr[1] : 0;
+}
+
 #if defined(__CUDACC__)
 __device__ __forceinline__ unsigned res_ld_acquire(const unsigned* p) {
     unsigned v;
@@ -140,6 +157,214 @@ resident_kernel(const PassArgs a1, const PassArgs a2, const ResidentArgs r) {
             }
         }
     }
+}
+
+// ---- software-pipelined variant ---------------------------------------------
+// While a CTA computes tile k, the inputs of tile k+1 are already on their way
+// into a shared-memory staging buffer (cp.async, 16 points per thread in slots
+// private to the thread, so the staged data needs no barrier): the first
+// sub-stage of every tile reads shared memory instead of waiting on global
+// latency.  The next item is claimed one item ahead; its prefetch is issued
+// right after the current tile's first barrier -- for a pass-2 tile only when
+// one poll shows its transform's pass 1 complete, otherwise the tile is loaded
+// (after a bounded wait) once the current tile is published.
+
+template <typename T>
+__device__ __forceinline__ void res_cp_async(C2<T>* dst, const C2<T>* src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(C2<T>) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void res_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void res_cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Issue the loads of global tile g of the pass L (arguments a) into the
+// staging slots of this thread; threads t < J also record the tile's lines.
+template <typename L, typename T>
+__device__ __forceinline__ void res_prefetch(const PassArgs& a, long long g, C2<T>* stage, LeanLine* lines) {
+    const int t = threadIdx.x;
+    long long bin, bout, j;
+    int i;
+    resident_line(a, L::LOGJ, L::LOGR_, g, t, bin, bout, j, i);
+    if (t < L::J) lines[t] = LeanLine{bin, bout, j};
+    const long long rs = a.in_estride << a.logNj;
+    const C2<T>* src = (const C2<T>*)a.in + bin + j * a.in_estride + (long long)i * rs;
+    const long long s16 = rs << (L::LOGR_ - 4);
+#pragma unroll
+    for (int m = 0; m < 16; ++m) res_cp_async<T>(&stage[m * L::THREADS + t], src + m * s16);
+    res_cp_commit();
+}
+
+// One tile of pass L from the staging buffer.  pre(): run by every thread just
+// before the first barrier; post(): just after it.
+template <typename L, typename T, typename Pre, typename Post>
+__device__ __forceinline__ void res_pf_tile(const PassArgs& a, const TwTables<T>* tw, C2<T>* sm, const C2<T>* stage,
+                                            const LeanLine* lines, Pre pre, Post post) {
+    using V = C2<T>;
+    const int t = threadIdx.x;
+    int l, i;
+    lean_map<true, L::LOGJ>(t, L::LOGR_ - 4, l, i);
+    const long long j = lines[l].j;
+    V v[16];
+    res_cp_wait_all();
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = stage[m * L::THREADS + t];
+    if (a.conj_in) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
+    }
+    L::pre_twiddle_dft(a, tw, j, i, v);
+    L::template write_smem<0>(sm, l, i, v);
+    pre();
+    __syncthreads();
+    if (a.discard_in) {
+        // every load of the tile has completed: drop the scratch lines just read
+        constexpr int PER_LINE = 128 / (int)sizeof(V);
+        if (L::J >= PER_LINE && (l % PER_LINE) == 0) {
+            const LeanLine ln = lines[l];
+            const V* src = (const V*)a.in + ln.bin + ln.j * a.in_estride;
+            const long long rs = a.in_estride << a.logNj;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) discard_l2(&src[(long long)(i + (m << (L::LOGR_ - 4))) * rs]);
+        }
+    }
+    post();
+    if constexpr (L::NS >= 3) {
+        constexpr int S = 1;
+        constexpr int RHO = 1 << LeanSched<L::LOGR_>::lr[S];
+        V w[16];
+        int ls[16 / RHO], is[16 / RHO];
+#pragma unroll
+        for (int q = 0; q < 16 / RHO; ++q) L::template read<S, L::COLL>(sm, t, q, &w[q * RHO], ls[q], is[q]);
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 16 / RHO; ++q) {
+            L::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
+            L::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
+        }
+        __syncthreads();
+    }
+    {
+        constexpr int S = L::NS - 1;
+        constexpr int RHO = 1 << LeanSched<L::LOGR_>::lr[S];
+        V w[16];
+        int ls[16 / RHO], is[16 / RHO];
+#pragma unroll
+        for (int q = 0; q < 16 / RHO; ++q) L::template read<S, true>(sm, t, q, &w[q * RHO], ls[q], is[q]);
+#pragma unroll
+        for (int q = 0; q < 16 / RHO; ++q) {
+            L::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
+            L::template write_global<S>(a, tw, lines, ls[q], is[q], &w[q * RHO]);
+        }
+    }
+}
+
+template <typename T, int R1, int R2, int LOGT>
+constexpr size_t resident_pf_smem_bytes() {
+    using L1 = Lean<T, R1, LOGT, true, false, LD_C, ST_C>;
+    using L2 = Lean<T, R2, LOGT, true, true, LD_C, ST_C>;
+    constexpr int ex = L1::SMEM_ELEMS > L2::SMEM_ELEMS ? L1::SMEM_ELEMS : L2::SMEM_ELEMS;
+    constexpr int jm = L1::J > L2::J ? L1::J : L2::J;
+    return sizeof(C2<T>) * ((size_t)ex + 16 * (size_t)(1 << LOGT)) + 2 * sizeof(LeanLine) * (size_t)jm;
+}
+// CTAs per SM the shared memory allows (227 KB per CTA at most, 228 KB per SM).
+template <typename T, int R1, int R2, int LOGT>
+constexpr int resident_pf_min_blocks() {
+    constexpr size_t per = resident_pf_smem_bytes<T, R1, R2, LOGT>() + 1024;
+    constexpr int by_smem = (int)((228u * 1024u) / per);
+    constexpr int by_regs = LOGT <= 7 ? 4 : (LOGT == 8 ? 2 : 1);
+    return by_smem < 1 ? 1 : (by_smem < by_regs ? by_smem : by_regs);
+}
+
+template <typename T, int R1, int R2, int LOGT>
+__global__ void __launch_bounds__(1 << LOGT, (resident_pf_min_blocks<T, R1, R2, LOGT>()))
+resident_pf_kernel(const PassArgs a1, const PassArgs a2, const ResidentArgs r) {
+    using L1 = Lean<T, R1, LOGT, true, false, LD_C, ST_C>;
+    using L2 = Lean<T, R2, LOGT, true, true, LD_C, ST_C>;
+    using V = C2<T>;
+    constexpr int TH = 1 << LOGT;
+    constexpr int EX = L1::SMEM_ELEMS > L2::SMEM_ELEMS ? L1::SMEM_ELEMS : L2::SMEM_ELEMS;
+    constexpr int JM = L1::J > L2::J ? L1::J : L2::J;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    V* sm = (V*)smraw;
+    V* stage = sm + EX;
+    LeanLine* lbuf = (LeanLine*)(stage + 16 * TH);
+    // [c]: the current item of a tile of parity c; [c ^ 1]: written by thread 0
+    // during that tile (the next item), so the two never race
+    __shared__ long long s_next[2];   // item, -1: none
+    __shared__ int s_pf[2];           // its loads are already in flight
+    __shared__ int s_go;
+    const TwTables<T>* tw = (const TwTables<T>*)a1.tw;
+    const int t = threadIdx.x;
+    const int lt = r.log_tiles;
+    const long long nitems = r.B << (lt + 1);
+    unsigned long long claim = 0;   // thread 0: the item after s_next, in flight
+    if (t == 0) {
+        const long long c0 = atomicAdd(&r.ctr[0], 1u);
+        s_next[0] = c0 < nitems ? c0 : -1;
+        if (s_next[0] >= 0) claim = atomicAdd(&r.ctr[0], 1u);
+        s_pf[0] = 0;
+    }
+    __syncthreads();
+    int cur_buf = 0;
+    for (;;) {
+        const long long item = s_next[cur_buf];
+        const int prefetched = s_pf[cur_buf];
+        if (item < 0) break;
+        int pass;
+        long long tr, tile;
+        resident_decode(item, r.B, r.lag, lt, pass, tr, tile);
+        LeanLine* lines = lbuf + cur_buf * JM;
+        if (!prefetched) {
+            // not prefetched: wait for its dependency, then load it now
+            if (t == 0) s_go = (pass == 2) ? resident_wait(r, tr, 1u << lt, item) : !res_ld_relaxed(&r.ctr[1]);
+            __syncthreads();
+            if (!s_go) break;
+            if (pass == 1) res_prefetch<L1, T>(a1, (tr << lt) + tile, stage, lines);
+            else res_prefetch<L2, T>(a2, (tr << lt) + tile, stage, lines);
+            __syncthreads();   // lines of the tile
+        }
+        LeanLine* nlines = lbuf + (cur_buf ^ 1) * JM;
+        // thread 0, before the tile's first barrier: take the next claim, and
+        // check (one poll) whether its loads may start now
+        const int nb = cur_buf ^ 1;
+        auto pre = [&]() {
+            if (t == 0) {
+                const long long c = (long long)claim;
+                const long long nx = (c < nitems && !res_ld_relaxed(&r.ctr[1])) ? c : -1;
+                int pf = 0;
+                if (nx >= 0) {
+                    claim = atomicAdd(&r.ctr[0], 1u);
+                    int p2;
+                    long long tr2, tile2;
+                    resident_decode(nx, r.B, r.lag, lt, p2, tr2, tile2);
+                    pf = (p2 == 1) || res_ld_acquire(&r.ctr[2 + tr2]) >= (1u << lt);
+                }
+                s_next[nb] = nx;
+                s_pf[nb] = pf;
+            }
+        };
+        auto post = [&]() {
+            if (s_pf[nb]) {
+                int p2;
+                long long tr2, tile2;
+                resident_decode(s_next[nb], r.B, r.lag, lt, p2, tr2, tile2);
+                if (p2 == 1) res_prefetch<L1, T>(a1, (tr2 << lt) + tile2, stage, nlines);
+                else res_prefetch<L2, T>(a2, (tr2 << lt) + tile2, stage, nlines);
+            }
+        };
+        if (pass == 1) res_pf_tile<L1, T>(a1, tw, sm, stage, lines, pre, post);
+        else res_pf_tile<L2, T>(a2, tw, sm, stage, lines, pre, post);
+        __syncthreads();
+        if (pass == 1 && t == 0) {
+            __threadfence();
+            atomicAdd(&r.ctr[2 + tr], 1u);
+        }
+        cur_buf ^= 1;
+    }
+    res_cp_wait_all();
 }
 #endif
 

@@ -9,7 +9,9 @@ namespace nfft {
 void resident_register_a(std::vector<ResidentEntry>& v) {
 #define X(R1, R2, LT)                                                                                  \
     v.push_back(ResidentEntry{R1, R2, LT, (const void*)resident_kernel<real_t, R1, R2, LT>,            \
-                              resident_smem_bytes<real_t, R1, R2, LT>()});
+                              resident_smem_bytes<real_t, R1, R2, LT>(),                                \
+                              (const void*)resident_pf_kernel<real_t, R1, R2, LT>,                      \
+                              resident_pf_smem_bytes<real_t, R1, R2, LT>()});
     NFFT_RESIDENT_A(X)
 #undef X
 }

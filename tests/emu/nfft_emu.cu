@@ -713,7 +713,7 @@ long long launch_count() { return g_launches; }
 static std::vector<ResidentEntry>& emu_resident_registry() {
     static std::vector<ResidentEntry> v = [] {
         std::vector<ResidentEntry> r;
-#define X(R1, R2, LT) r.push_back(ResidentEntry{R1, R2, LT, nullptr, 0});
+#define X(R1, R2, LT) r.push_back(ResidentEntry{R1, R2, LT, nullptr, 0, nullptr, 0});
         NFFT_RESIDENT_A(X) NFFT_RESIDENT_B(X)
 #undef X
         return r;
@@ -755,6 +755,26 @@ bool launch_resident(const DeviceCtx*, const PassArgs& a1, const PassArgs& a2, i
         if (tr < 0 || tr >= B || tile < 0 || tile >= T) {
             fprintf(stderr, "nfft_emu: resident item %lld decodes outside the launch\n", g);
             abort();
+        }
+        {
+            // the prefetching kernel's per-thread line and source addresses
+            const PassArgs& a = pass == 1 ? a1 : a2;
+            const int logR = pass == 1 ? r1 : r2, logJ = e->logt + 4 - logR;
+            const long long gt = (tr << lt) + tile;
+            for (int t = 0; t < (1 << e->logt); ++t) {
+                long long bin, bout, j, tmp[3];
+                int i;
+                resident_line(a, logJ, logR, gt, t, bin, bout, j, i);
+                TileLines tl{&tmp[0], &tmp[1], &tmp[2]};
+                line_setup(a, (gt << logJ) + (t & ((1 << logJ) - 1)), 0, tl);
+                if (bin != tmp[0] || bout != tmp[1] || j != tmp[2] || i != (t >> logJ)) {
+                    fprintf(stderr, "nfft_emu: resident line of thread %d differs from line_setup\n", t);
+                    abort();
+                }
+                const long long rs = a.in_estride << a.logNj;
+                const cplx_t* src = (const cplx_t*)a.in + bin + j * a.in_estride + (long long)i * rs;
+                for (int m = 0; m < 16; ++m) nfft_emu_check(src + m * (rs << (logR - 4)), sizeof(cplx_t), 0);
+            }
         }
         if (pass == 2) {
             if (done[tr] != T) {
