@@ -224,6 +224,240 @@ def bench_float_forms(args, wl, x64, stream, ms_fp64, rank, world, dist):
     return out
 
 
+def _uneven_config(count, seed, nmax=1 << 18):
+    """Kinds and lengths of the ragged-batch configuration: N log-uniform on
+    [16, nmax], 80% powers of two, the rest split between primes and composite
+    lengths; 50% c2c / 30% realdft / 20% DCT-2 (seeded)."""
+    import numpy as np
+
+    def is_prime(n):
+        if n < 2:
+            return False
+        i = 2
+        while i * i <= n:
+            if n % i == 0:
+                return False
+            i += 1
+        return True
+
+    rng = np.random.default_rng(seed)
+    kinds, Ns = [], []
+    lo, hi = math.log2(16), math.log2(nmax)
+    for _ in range(count):
+        u = rng.random()
+        kind = "dft" if u < 0.5 else ("realdft" if u < 0.8 else "dct2")
+        e = rng.uniform(lo, hi)
+        v = rng.random()
+        if v < 0.8:
+            n = 1 << int(round(e))
+        else:
+            n = max(17, int(round(2 ** e)))
+            if v < 0.9:
+                while not is_prime(n):
+                    n += 1
+            else:
+                if n & (n - 1) == 0:
+                    n += 1
+                while is_prime(n) or n & (n - 1) == 0:
+                    n += 1
+        kinds.append(kind)
+        Ns.append(n)
+    return kinds, Ns
+
+
+def bench_configs(args, stream):
+    """The other configurations of the reference's benchmark set on this GPU:
+    time per call (CUDA events, warm, median; L2 flushed before every timed
+    call), algorithmic GB/s (one read of the input and one write of the output
+    per transform) and the largest relative L2 error of a sample against an
+    independent FP64 FFT (torch / scipy)."""
+    import numpy as np
+    import scipy.fft as sf
+    import torch
+
+    from notorious_fft import FORM_SPLIT_TC, load
+
+    Ld, Lf = load(single=False), load(single=True)
+    Ld.set_stream(stream.cuda_stream)
+    Lf.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    steps = max(3, min(args.steps, 7))
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20261203)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for _ in range(steps):
+            flush.fill_(1)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    def uni(*shape, dt=torch.float64):
+        return torch.rand(*shape, generator=g, device="cuda", dtype=dt) * 2 - 1
+
+    def cuni(*shape, dt=torch.complex128):
+        r = torch.float64 if dt == torch.complex128 else torch.float32
+        return torch.complex(uni(*shape, dt=r), uni(*shape, dt=r))
+
+    def rel(a, b):
+        a, b = np.asarray(a, dtype=np.complex128), np.asarray(b, dtype=np.complex128)
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    out = {}
+
+    def entry(name, ms, nbytes, err, **kw):
+        e = {"ms": round(ms, 4), "gb_s": round(nbytes / (ms * 1e-3) / 1e9, 1), "max_rel_l2": err}
+        e.update(kw)
+        out[name] = e
+
+    # C1: 256 x 4096 FP64 dft + invdft (fits L2: flushed before every call)
+    x = cuni(256, 4096)
+    y, z = torch.empty_like(x), torch.empty_like(x)
+    with Ld.mkaux("dft", [4096]) as a:
+        ms = timed(lambda: (a.batched("dft", x, y, 256, 4096, 4096), a.batched("invdft", y, z, 256, 4096, 4096)))
+        torch.cuda.synchronize()
+        err = rel(y[:4].cpu(), torch.fft.fft(x[:4], dim=1).cpu())
+    entry("c1_dft_invdft_4096x256_f64", ms, 2 * 256 * 4096 * 32, err)
+    del x, y, z
+
+    # C2: realdft 2^20 x 16
+    n = 1 << 20
+    x = uni(16, n)
+    zc = torch.empty(16, n // 2 + 1, dtype=torch.complex128, device="cuda")
+    with Ld.mkaux("realdft", [n]) as a:
+        ms = timed(lambda: a.batched("realdft", x, zc, 16, n, n // 2 + 1))
+        torch.cuda.synchronize()
+        err = rel(zc[:2].cpu(), torch.fft.rfft(x[:2], dim=1).cpu())
+    entry("c2_realdft_1048576x16_f64", ms, 16 * (n * 8 + (n // 2 + 1) * 16), err)
+    del x, zc
+    # C2: DCT-2 / DST-2 / DCT-4, 8192 x 512
+    n, b = 8192, 512
+    x = uni(b, n)
+    y = torch.empty_like(x)
+    for kind, fam, ref in (("dct2", "t2t3", lambda v: sf.dct(v, 2)), ("dst2", "t2t3", lambda v: sf.dst(v, 2)),
+                           ("dct4", "t4", lambda v: sf.dct(v, 4))):
+        with Ld.mkaux(fam, [n]) as a:
+            ms = timed(lambda: a.batched(kind, x, y, b, n, n))
+            torch.cuda.synchronize()
+            xs, ys = x[:2].cpu().numpy(), y[:2].cpu().numpy()
+            err = max(rel(ys[i], ref(xs[i])) for i in range(2))
+        entry(f"c2_{kind}_8192x512_f64", ms, b * n * 16, err)
+    del x, y
+    # C2: 2-D 2048^2 and 3-D 256^3 complex
+    for dims in ((2048, 2048), (256, 256, 256)):
+        x = cuni(*dims)
+        y = torch.empty_like(x)
+        with Ld.mkaux("dft", list(dims)) as a:
+            ms = timed(lambda: a("dft", x, y))
+            torch.cuda.synchronize()
+            err = rel(y.cpu(), torch.fft.fftn(x).cpu())
+        entry("c2_dft_" + "x".join(map(str, dims)) + "_f64", ms, x.numel() * 32, err)
+        del x, y
+    # C2: Bluestein, N = 1,000,003 x 4
+    n = 1000003
+    x = cuni(4, n)
+    y = torch.empty_like(x)
+    with Ld.mkaux("dft", [n]) as a:
+        ms = timed(lambda: a.batched("dft", x, y, 4, n, n))
+        torch.cuda.synchronize()
+        err = rel(y[:1].cpu(), torch.fft.fft(x[:1], dim=1).cpu())
+    entry("c2_bluestein_dft_1000003x4_f64", ms, 4 * n * 32, err)
+    del x, y
+
+    # C3: split tensor-core FP32 form, N = 2^16, 10% of the transforms x 1e4
+    n, b = 1 << 16, 1024
+    x = cuni(b, n, dt=torch.complex64)
+    sel = torch.randperm(b, generator=torch.Generator().manual_seed(3))[: b // 10].cuda()
+    x[sel] *= 1e4
+    y = torch.empty_like(x)
+    x64 = x[:64].to(torch.complex128)
+    ref = torch.fft.fft(x64, dim=1)
+    for name, form in (("fp32_plain", 0), ("split_tc", FORM_SPLIT_TC)):
+        with Lf.mkaux("dft", [n]) as a:
+            a.set_form(form)
+            ms = timed(lambda: a.batched("dft", x, y, b, n, n))
+            torch.cuda.synchronize()
+            d = (y[:64].to(torch.complex128) - ref)
+            errs = torch.linalg.vector_norm(d, dim=1) / torch.linalg.vector_norm(ref, dim=1)
+        entry(f"c3_{name}_65536x{b}_scaled10pct", ms, b * n * 16, float(errs.max().item()),
+              transforms_per_s=round(b / (ms * 1e-3), 1), scaled_in_sample=int((sel < 64).sum().item()))
+    del x, y, x64, ref
+
+    # C4: ragged batch of 20,000 transforms, one persistent launch (CUDA graph)
+    kinds, Ns = _uneven_config(20000, seed=2026)
+    for L, tag, rs in ((Ld, "f64", 8), (Lf, "f32", 4)):
+        t0 = time.perf_counter()
+        bt = L.mkbatch(kinds, Ns)
+        build_s = time.perf_counter() - t0
+        dt = torch.float64 if rs == 8 else torch.float32
+        xi = uni(bt.in_size, dt=dt)
+        yo = torch.empty(bt.out_size, dtype=dt, device="cuda")
+        ms = timed(lambda: bt.execute(xi, yo))
+        assert bt.status() == 0
+        nbytes = 0
+        for k, nn in zip(kinds, Ns):
+            ci = 2 * nn if k == "dft" else nn
+            co = 2 * nn if k == "dft" else (2 * (nn // 2 + 1) if k == "realdft" else nn)
+            nbytes += (ci + co) * rs
+        # error sample: the first c2c transform of the packed layout
+        i0 = kinds.index("dft")
+        off = 0
+        for k, nn in zip(kinds[:i0], Ns[:i0]):
+            off += 2 * nn if k == "dft" else nn
+            off += off & 1
+        ooff = 0
+        for k, nn in zip(kinds[:i0], Ns[:i0]):
+            ooff += 2 * nn if k == "dft" else (2 * (nn // 2 + 1) if k == "realdft" else nn)
+            ooff += ooff & 1
+        n0 = Ns[i0]
+        xin = xi[off: off + 2 * n0].double().view(n0, 2)
+        got = yo[ooff: ooff + 2 * n0].double().view(n0, 2)
+        refc = torch.fft.fft(torch.complex(xin[:, 0], xin[:, 1]))
+        err = rel(torch.complex(got[:, 0], got[:, 1]).cpu(), refc.cpu())
+        info = bt.info()
+        bt.free()
+        entry(f"c4_ragged_20000_{tag}", ms, nbytes, err, transforms_per_s=round(20000 / (ms * 1e-3), 1),
+              build_s=round(build_s, 2), items=info["items"], tiles=info["tiles"], ctas=info["ctas"],
+              launches_per_call=1, graph=True)
+        del xi, yo
+
+    # C5: one forward + backward step of L = sum w |rfft2(x)|^2 + sum v DCT2(rowmean(x)), x 64 x 512 x 512 FP32
+    B5, N1, N2 = 64, 512, 512
+    x = torch.randn(B5, N1, N2, generator=g, device="cuda", dtype=torch.float32)
+    w = torch.rand(B5, N1, N2 // 2 + 1, generator=g, device="cuda", dtype=torch.float32) + 0.5
+    v = torch.rand(B5, N1, generator=g, device="cuda", dtype=torch.float32) + 0.5
+    rf, dc = Lf.mkaux("realdft", [N1, N2]), Lf.mkaux("t2t3", [N1])
+    zz = torch.empty(B5, N1, N2 // 2 + 1, dtype=torch.complex64, device="cuda")
+    gx = torch.empty_like(x)
+    dd, gm = torch.empty(B5, N1, device="cuda"), torch.empty(B5, N1, device="cuda")
+
+    def step5():
+        rf.batched("realdft", x, zz, B5, N1 * N2, N1 * (N2 // 2 + 1))
+        m = x.mean(dim=2)
+        dc.batched("dct2", m, dd, B5, N1, N1)
+        loss = (w * (zz.real ** 2 + zz.imag ** 2)).sum() + (v * dd).sum()
+        gz = (2 * w) * zz
+        rf.vjp_batched("realdft", gz, gx, B5, N1 * (N2 // 2 + 1), N1 * N2)
+        dc.vjp_batched("dct2", v, gm, B5, N1, N1)
+        gx.add_(gm.unsqueeze(2) / N2)
+        return loss
+
+    ms = timed(step5)
+    rf.free()
+    dc.free()
+    entry("c5_loss_forward_backward_64x512x512_f32", ms, 2 * (x.numel() * 4 + zz.numel() * 8), None,
+          note="realdft 2-D + DCT-2 forward, their adjoint kernels backward, torch elementwise glue")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -235,6 +469,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the float-library forms")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations (C1-C5)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.batch:
@@ -329,6 +564,10 @@ def main():
     if not args.no_forms:
         forms = bench_float_forms(args, wl, x, stream, ms_step, rank, world, dist)
 
+    configs = None
+    if not args.no_configs and rank == 0 and world == 1:
+        configs = bench_configs(args, stream)
+
     e2e = None
     if not args.no_e2e and rank == 0 and world == 1:
         xh = x.cpu().pin_memory()
@@ -366,6 +605,8 @@ def main():
             "clocks": ck, "round_trip_rel_err": err,
         }
         line.update(forms)
+        if configs is not None:
+            line["configs"] = configs
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
