@@ -5,8 +5,9 @@
 // passes (nfft_pass.cuh), with the transform family's pre/post operators fused
 // into the first and last pass.  Power-of-two axes use the passes directly;
 // other complex axes use Bluestein (chirp premultiply fused into the first
-// forward pass, filter product + first inverse pass fused into the last
-// forward pass, window + chirp postmultiply fused into the last inverse pass).
+// forward pass, the filter product into the first inverse pass -- or, when the
+// padded length fits one tile, the whole convolution in one pass -- and window
+// + chirp postmultiply into the last inverse pass).
 #pragma once
 
 #include <cuda_runtime.h>

@@ -34,9 +34,10 @@ using PassFn = void (*)(const PassArgs);
     X(LD_R2C, ST_C)            \
     X(LD_R2C, ST_R)            \
     X(LD_C, ST_C2R)            \
-    X(LD_IR, ST_C2R)
+    X(LD_IR, ST_C2R)           \
+    X(LD_FILT, ST_C)
 
-constexpr int NLOAD = 7, NSTORE = 7;
+constexpr int NLOAD = NUM_LOAD_OPS, NSTORE = NUM_STORE_OPS;
 
 static PassFn pass_table(int log_tile, int ld, int st) {
     static PassFn t12[NLOAD][NSTORE] = {};

@@ -49,4 +49,17 @@
     X(4, 7, 1, 1, LD_C, ST_C) X(5, 7, 1, 1, LD_C, ST_C) X(6, 7, 1, 1, LD_C, ST_C)                  \
     X(7, 7, 1, 1, LD_C, ST_C) X(8, 7, 1, 1, LD_C, ST_C) X(9, 7, 1, 1, LD_C, ST_C)
 
-#define NFFT_LEAN_ALL(X) NFFT_LEAN_C2C(X) NFFT_LEAN_REAL(X) NFFT_LEAN_MULTI(X) NFFT_LEAN_C2C_T7(X)
+// multi-pass Bluestein: chirp premultiply (first forward pass), filter product
+// (first inverse pass), window + chirp postmultiply (last inverse pass)
+#define NFFT_LEAN_BLUE(X)                                                                          \
+    X(5, 8, 1, 0, LD_BLUE, ST_C) X(6, 8, 1, 0, LD_BLUE, ST_C) X(7, 8, 1, 0, LD_BLUE, ST_C)         \
+    X(8, 8, 1, 0, LD_BLUE, ST_C) X(9, 8, 1, 0, LD_BLUE, ST_C) X(10, 8, 1, 0, LD_BLUE, ST_C)        \
+    X(11, 9, 1, 0, LD_BLUE, ST_C)                                                                  \
+    X(5, 8, 1, 0, LD_FILT, ST_C) X(6, 8, 1, 0, LD_FILT, ST_C) X(7, 8, 1, 0, LD_FILT, ST_C)         \
+    X(8, 8, 1, 0, LD_FILT, ST_C) X(9, 8, 1, 0, LD_FILT, ST_C) X(10, 8, 1, 0, LD_FILT, ST_C)        \
+    X(11, 9, 1, 0, LD_FILT, ST_C)                                                                  \
+    X(4, 8, 1, 1, LD_C, ST_BLUE) X(5, 8, 1, 1, LD_C, ST_BLUE) X(6, 8, 1, 1, LD_C, ST_BLUE)         \
+    X(7, 8, 1, 1, LD_C, ST_BLUE) X(8, 8, 1, 1, LD_C, ST_BLUE) X(9, 8, 1, 1, LD_C, ST_BLUE)         \
+    X(10, 8, 1, 1, LD_C, ST_BLUE) X(11, 9, 1, 1, LD_C, ST_BLUE)
+
+#define NFFT_LEAN_ALL(X) NFFT_LEAN_C2C(X) NFFT_LEAN_REAL(X) NFFT_LEAN_MULTI(X) NFFT_LEAN_C2C_T7(X) NFFT_LEAN_BLUE(X)

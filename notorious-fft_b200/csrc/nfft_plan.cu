@@ -678,11 +678,11 @@ static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const 
             cur = out;
             bi ^= 1;
         }
-        if (recorder()) {
-            // queue form: the last forward pass and the first inverse pass stay
-            // separate specialized passes; the filter product and conjugation
-            // are the inverse pass's load operator (one more sweep of M, no
-            // generic middle pass)
+        {
+            // the last forward pass and the first inverse pass stay separate
+            // specialized passes; the filter product and conjugation are the
+            // inverse pass's load operator (one more sweep of M than a fused
+            // middle pass, but every pass runs as a specialized kernel)
             View out = scratch_view(buf[bi], vs, M, false);
             if (!run_pass(c, cur, out, logM, logNs, f.plog[np - 1], f.tile[np - 1], f.nsub[np - 1], f.sub[np - 1], op,
                           false, false, 0, logNs, ax.chirp, ax.filt, s))
@@ -698,17 +698,8 @@ static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const 
                 return false;
             cur = out2;
             bi ^= 1;
-        } else {
-            // last forward pass + filter + first inverse pass
-            View out = scratch_view(buf[bi], vs, M, false);
-            OpSpec o = op;
-            if (!run_pass(c, cur, out, logM, logNs, f.plog[np - 1], f.tile[np - 1], f.nsub[np - 1], f.sub[np - 1], o,
-                          false, false, 1, 0, ax.chirp, ax.filt, s))
-                return false;
-            cur = out;
-            bi ^= 1;
         }
-        // remaining inverse passes (the first one was fused above)
+        // remaining inverse passes (the first one ran above)
         int logNs_inv = g.plog[0];
         for (int i = 1; i < np; ++i) {
             bool last = i == np - 1;

@@ -277,12 +277,13 @@ using EmuFn = void (*)(const PassArgs&, long long, long long);
 #define NFFT_PAIRS(X) \
     X(LD_C, ST_C) X(LD_C, ST_R) X(LD_C, ST_T2) X(LD_C, ST_T3) X(LD_C, ST_T4) X(LD_C, ST_BLUE) X(LD_T2, ST_C) \
     X(LD_T2, ST_T2) X(LD_T3, ST_C) X(LD_T3, ST_T3) X(LD_IR, ST_C) X(LD_T4, ST_C) X(LD_T4, ST_T4)          \
-    X(LD_BLUE, ST_C) X(LD_BLUE, ST_BLUE) X(LD_R2C, ST_C) X(LD_R2C, ST_R) X(LD_C, ST_C2R) X(LD_IR, ST_C2R)
+    X(LD_BLUE, ST_C) X(LD_BLUE, ST_BLUE) X(LD_R2C, ST_C) X(LD_R2C, ST_R) X(LD_C, ST_C2R) X(LD_IR, ST_C2R)   \
+    X(LD_FILT, ST_C)
 
 static long long g_launches = 0;
 
 bool launch_pass(const PassArgs& a, int ld, int st, int log_tile, long long ntiles, cudaStream_t) {
-    static EmuFn t12[7][7] = {}, t13[7][7] = {};
+    static EmuFn t12[NUM_LOAD_OPS][NUM_STORE_OPS] = {}, t13[NUM_LOAD_OPS][NUM_STORE_OPS] = {};
     static bool filled = false;
     if (!filled) {
 #define X(L, S) t12[L][S] = emu_pass<12, L, S>; t13[L][S] = emu_pass<13, L, S>;
