@@ -44,6 +44,8 @@ MEASURED_TRAFFIC_PER_TRANSFORM = {("c2c", 65536): 3.64e6}
 WORKLOADS = {
     "c2c": dict(N=65536, batch=4096, l2="inputs 4 GiB per array > L2 (no flush)", flush=False),
     "c1": dict(N=4096, batch=256, l2="L2 flushed (256 MiB write) between steps", flush=True),
+    # ragged batch in one persistent launch; `batch` = number of transforms
+    "ragged": dict(N=0, batch=20000, l2="L2 flushed (256 MiB write) between steps", flush=True),
 }
 
 
@@ -458,6 +460,48 @@ def bench_configs(args, stream):
     return out
 
 
+def run_ragged(args, wl):
+    """Profiling workload: one ragged batch (FP64) of `batch` transforms of the
+    uneven configuration, executed through the persistent queue."""
+    import torch
+
+    from notorious_fft import load
+
+    L = load(single=False)
+    stream = torch.cuda.current_stream()
+    L.set_stream(stream.cuda_stream)
+    kinds, Ns = _uneven_config(wl["batch"], seed=2026)
+    b = L.mkbatch(kinds, Ns)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    x = torch.rand(b.in_size, generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+    y = torch.empty(b.out_size, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        b.execute(x, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0.record(stream)
+        b.execute(x, y)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    assert b.status() == 0
+    nbytes = 0
+    for k, n in zip(kinds, Ns):
+        ci = 2 * n if k == "dft" else n
+        co = 2 * n if k == "dft" else (2 * (n // 2 + 1) if k == "realdft" else n)
+        nbytes += (ci + co) * 8
+    m = statistics.median(ms)
+    print(json.dumps({"workload": f"ragged fp64 x{wl['batch']}", "ms": round(m, 4),
+                      "gb_s": round(nbytes / (m * 1e-3) / 1e9, 1),
+                      "transforms_per_s": round(wl["batch"] / (m * 1e-3), 1), "info": b.info()}))
+    b.free()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -478,6 +522,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args, wl)
+    if args.workload == "ragged":
+        return run_ragged(args, wl)
 
     import numpy as np
     import torch
