@@ -386,8 +386,29 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
     }
 }
 
+// Minimum CTAs per SM the specialized kernels are compiled for (register
+// budget 65536 / (threads x CTAs)).  The passes are latency-bound, so warps per
+// SM matter; the float kernels fit more CTAs than the double ones.
+#ifndef NFFT_LEAN_MINB_T7_F64
+#define NFFT_LEAN_MINB_T7_F64 4
+#endif
+#ifndef NFFT_LEAN_MINB_T7_F32
+#define NFFT_LEAN_MINB_T7_F32 4
+#endif
+#ifndef NFFT_LEAN_MINB_T8_F64
+#define NFFT_LEAN_MINB_T8_F64 2
+#endif
+#ifndef NFFT_LEAN_MINB_T8_F32
+#define NFFT_LEAN_MINB_T8_F32 2
+#endif
+template <typename T, int LOGT>
+constexpr int lean_min_blocks() {
+    return LOGT <= 7 ? (sizeof(T) == 4 ? NFFT_LEAN_MINB_T7_F32 : NFFT_LEAN_MINB_T7_F64)
+                     : (LOGT == 8 ? (sizeof(T) == 4 ? NFFT_LEAN_MINB_T8_F32 : NFFT_LEAN_MINB_T8_F64) : 1);
+}
+
 template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
-__global__ void __launch_bounds__(1 << LOGT, (LOGT <= 7 ? 4 : (LOGT == 8 ? 2 : 1)))
+__global__ void __launch_bounds__(1 << LOGT, (lean_min_blocks<T, LOGT>()))
 lean_pass_kernel(const PassArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     lean_tile<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>(a, (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x,

@@ -311,8 +311,14 @@ notorious_fft_batch* batch_create(int count, const int* kinds, const int* Ns, co
             rec.launches.push_back(r);
         } else {
             std::vector<int> split = opt.force_split;
-            if (split.empty() && opt.use_tuned && pow2(bk.n)) tune_get(k, bk.n, split);
+            bool tuned = false;
+            if (split.empty() && opt.use_tuned && pow2(bk.n)) tuned = tune_get(k, bk.n, split);
             bk.plan = plan_create_queue(k, bk.n, split.empty() ? nullptr : split.data(), (int)split.size());
+            if (!bk.plan && tuned) {
+                // a cached split this build cannot execute: use the default schedule
+                clear_error();
+                bk.plan = plan_create_queue(k, bk.n, nullptr, 0);
+            }
             if (!bk.plan) return fail();
             const long long e0 = cnt == 1 ? 1 : 0;   // a single transform: its offset goes into the pointer
             const void* inp = (const void*)(IN_BASE + (uintptr_t)(e0 * in_off[bk.members[0]] * (long long)sizeof(real_t)));

@@ -200,3 +200,36 @@ def test_queue_structure(emu_d):
     # 8192 points = 2 tiles of 4096 per pass, two passes, one tile per item
     assert info["tiles"] == 3 * 2 * 2 and info["items"] == 12
     assert info["scratch_bytes"] >= 3 * 8192 * 16
+
+
+def test_unusable_cached_split_falls_back(tmp_path):
+    """A tune-cache entry for this device whose split the planner rejects is
+    ignored: the batch is planned with the default schedule."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cache = tmp_path / "tune.json"
+    cache.write_text('{"format": "notorious_fft tune cache 1", "entries": [\n'
+                     '{"device": "emulated sm_100 sm_100 driver 0", "key": "f64:dft:8192", "split": [1, 12], "us": 1.0}'
+                     '\n]}\n')
+    child = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from notorious_fft import Library
+L = Library(sys.argv[2])
+print(L.tune_lookup("dft", 8192))
+b = L.mkbatch(["dft"], [8192])
+x = np.random.default_rng(0).uniform(-1, 1, b.in_size); y = np.zeros(b.out_size)
+b.execute(x, y)
+xc = x[0::2] + 1j * x[1::2]
+print(float(np.abs((y[0::2] + 1j * y[1::2]) - np.fft.fft(xc)).max() / np.abs(np.fft.fft(xc)).max()))
+"""
+    env = dict(os.environ, NOTORIOUS_FFT_TUNE_CACHE=str(cache))
+    r = subprocess.run([sys.executable, "-c", child, os.path.join(root, "notorious-fft_b200"),
+                        os.path.join(root, "tests", "emu", "_build", "libnfft_emu_d.so")],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = r.stdout.strip().splitlines()
+    assert json.loads(lines[0]) == [1, 12]          # the entry was read
+    assert float(lines[1]) < 1e-14                   # and the batch ran on the default schedule
