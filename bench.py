@@ -374,6 +374,21 @@ def bench_configs(args, stream):
     entry("c2_bluestein_dft_1000003x4_f64", ms, 4 * n * 32, err)
     del x, y
 
+    # the batched c2c range of the FP64 roofline target: N = 2^12 .. 2^20, both
+    # precisions, 1 GiB per array, dft and invdft alternating
+    for L, tag, es in ((Ld, "f64", 16), (Lf, "f32", 8)):
+        for logn in range(12, 21):
+            n = 1 << logn
+            b = (1 << 30) // (n * es)
+            x = cuni(b, n, dt=torch.complex128 if es == 16 else torch.complex64)
+            y = torch.empty_like(x)
+            with L.mkaux("dft", [n]) as a:
+                ms = timed(lambda: a.batched("dft", x, y, b, n, n))
+                torch.cuda.synchronize()
+                err = rel(y[:1].cpu(), torch.fft.fft(x[:1].to(torch.complex128), dim=1).cpu())
+            entry(f"sweep_c2c_{tag}_n{n}", ms, b * n * 2 * es, err, batch=b)
+            del x, y
+
     # C3: split tensor-core FP32 form, N = 2^16, 10% of the transforms x 1e4
     n, b = 1 << 16, 1024
     x = cuni(b, n, dt=torch.complex64)

@@ -75,6 +75,40 @@ struct LeanLine {
     long long bin, bout, j;
 };
 
+// ---- mirror tiles: the last pass of a multi-pass realdft / DCT-2 / DST-2 ------
+// The last pass of the packed N/2-point spectrum Z (M = N/2) writes, for line j
+// of the ns = M / R lines of a transform, Z[j + r ns], r < R.  Bin k pairs with
+// bin M - k, which lives on line ns - j (lines 0 and ns / 2 pair with
+// themselves).  A mirror tile therefore holds J/2 "low" lines and their J/2
+// partners: tile tt of a transform holds j = tt J/2 + l and ns - (tt J/2 + l)
+// for l < J/2, except tile 0, whose first low line is j = 0 and first high line
+// j = ns / 2.  The Hermitian unpack then runs inside the tile.
+//
+// Stockham line of local line l (of J) in tile tt of a transform.
+NFFT_HD long long mirror_line(long long tt, int l, int J, long long ns) {
+    const int h = J / 2;
+    if (l < h) return (tt == 0 && l == 0) ? 0 : tt * h + l;
+    const int u = l - h;
+    if (tt == 0) return u == 0 ? ns / 2 : ns - u;
+    return ns - (tt * h + u);
+}
+// Local line of Stockham line j in tile tt (inverse of mirror_line).
+NFFT_HD int mirror_local(long long tt, long long j, int J, long long ns) {
+    const int h = J / 2;
+    if (tt == 0) {
+        if (j == 0) return 0;
+        if (j == ns / 2) return h;
+        return j < ns / 2 ? (int)j : (int)(h + (ns - j));
+    }
+    return j < ns / 2 ? (int)(j - tt * h) : (int)(h + (ns - j - tt * h));
+}
+// Bin k of unpack item (l < J/2, r < R) of tile tt: every item emits bins k and
+// M - k (unpack_pair), the items of a tile cover both lines of each pair.
+NFFT_HD long long mirror_item_k(long long tt, int l, int r, int R, long long ns, long long lowj) {
+    if (tt == 0 && l == 0) return r < R / 2 ? (long long)r * ns : ns / 2 + (long long)(r - R / 2) * ns;
+    return lowj + (long long)r * ns;
+}
+
 template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
 struct Lean {
     static constexpr int THREADS = 1 << LOGT;
@@ -89,7 +123,11 @@ struct Lean {
     static constexpr int NS = LeanSched<LOGR>::n;
     static constexpr int SMEM_ELEMS = lean_smem_elems<COLL, LOGR, LOGJ>();
     static_assert(LOGJ >= 0 && LOGJ <= 8, "tile must hold 1..256 lines");
-    static_assert(!(PAIRED && (COL_IN || COL_OUT)), "paired operators need whole contiguous lines");
+    // paired stores need whole lines in the tile: row tiles, or mirror tiles
+    // (column in and out) for the last pass of a multi-pass transform
+    static constexpr bool MIRROR = PAIRED && COL_IN && COL_OUT;
+    static_assert(!(PAIRED && (COL_IN != COL_OUT)), "paired operators need row tiles or mirror tiles");
+    static_assert(!MIRROR || LOGJ >= 1, "mirror tiles pair lines");
 
     // ---- first sub-stage: global -> registers -> radix 16 --------------------
     static NFFT_HD void first(const PassArgs& a, const TwTables<T>* tw, const LeanLine* lines, int t, C2<T>* v, int& l,
@@ -293,7 +331,13 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
     if (t < L::J) {
         long long tmp[3];
         TileLines tl{&tmp[0], &tmp[1], &tmp[2]};
-        line_setup(a, line0 + t, 0, tl);
+        if constexpr (L::MIRROR) {
+            const long long ns = 1ll << a.logNj, tpt = ns >> L::LOGJ;   // lines, tiles per transform
+            const long long tr = tile / tpt, tt = tile - tr * tpt;
+            line_setup(a, tr * ns + mirror_line(tt, t, L::J, ns), 0, tl);
+        } else {
+            line_setup(a, line0 + t, 0, tl);
+        }
         lines[t] = LeanLine{tmp[0], tmp[1], tmp[2]};
     }
     __syncthreads();
@@ -311,7 +355,7 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
     } else {
         L::template write_smem<0>(sm, l, i, v);
         __syncthreads();
-        if constexpr (LOAD == LD_C && COL_IN) {
+        if constexpr (LOAD == LD_C && COL_IN && !L::MIRROR) {   // mirror tiles: lines are not one address run
             // every load of the tile has completed: drop the scratch lines just read
             constexpr int PER_LINE = 128 / (int)sizeof(V);
             if (a.discard_in && L::J >= PER_LINE && (l % PER_LINE) == 0) {
@@ -372,7 +416,24 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
             }
         }
     }
-    if constexpr (L::PAIRED) {
+    if constexpr (L::MIRROR) {
+        __syncthreads();
+        // mirror tile: (J/2 low lines) x R unpack items, each emitting bins k, M - k
+        const long long ns = 1ll << a.logNj, tpt = ns >> L::LOGJ;
+        const long long tt = tile - (tile / tpt) * tpt;
+        const long long M = ns << LOGR;
+        constexpr int ITEMS = (L::J / 2) << LOGR;
+        for (int w = t; w < ITEMS; w += L::THREADS) {
+            const int l = w >> LOGR, r = w & ((1 << LOGR) - 1);
+            const LeanLine ln = lines[l];
+            const long long k = mirror_item_k(tt, l, r, 1 << LOGR, ns, ln.j);
+            unpack_pair<T, STORE>(a, tw, ln.bout, k, M, [&](long long q) {
+                const long long j = q & (ns - 1);
+                const int rr = (int)(q >> a.logNj);
+                return sm[NFFT_SM((lean_idx<true, LOGR, L::LOGJ>(mirror_local(tt, j, L::J, ns), rr)))];
+            });
+        }
+    } else if constexpr (L::PAIRED) {
         __syncthreads();
         // whole lines in row layout: realdft unpack / DCT-2 post pairs
         constexpr int ITEMS = (LOGR == 0) ? L::J : (L::J << (LOGR - 1));

@@ -29,11 +29,13 @@
     NFFT_LEAN_REAL_ONE(X, 10, 8) NFFT_LEAN_REAL_ONE(X, 11, 8) NFFT_LEAN_REAL_ONE(X, 12, 8)         \
     NFFT_LEAN_REAL_ONE(X, 13, 9)
 
-// first / last passes of multi-pass real transforms
+// first / last passes of multi-pass real transforms (the realdft / DCT-2 last
+// passes unpack in mirror tiles)
 #define NFFT_LEAN_MULTI_ONE(X, R, T)                                                               \
     X(R, T, 1, 0, LD_R2C, ST_C) X(R, T, 1, 0, LD_IR, ST_C) X(R, T, 1, 0, LD_T2, ST_C)             \
     X(R, T, 1, 0, LD_T3, ST_C) X(R, T, 1, 0, LD_T4, ST_C) X(R, T, 1, 1, LD_C, ST_C2R)             \
-    X(R, T, 1, 1, LD_C, ST_T3) X(R, T, 1, 1, LD_C, ST_T4)
+    X(R, T, 1, 1, LD_C, ST_T3) X(R, T, 1, 1, LD_C, ST_T4) X(R, T, 1, 1, LD_C, ST_R)              \
+    X(R, T, 1, 1, LD_C, ST_T2)
 #define NFFT_LEAN_MULTI(X)                                                                         \
     NFFT_LEAN_MULTI_ONE(X, 5, 8) NFFT_LEAN_MULTI_ONE(X, 6, 8) NFFT_LEAN_MULTI_ONE(X, 7, 8)         \
     NFFT_LEAN_MULTI_ONE(X, 8, 8) NFFT_LEAN_MULTI_ONE(X, 9, 8) NFFT_LEAN_MULTI_ONE(X, 10, 8)        \

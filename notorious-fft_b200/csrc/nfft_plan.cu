@@ -510,7 +510,16 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
     long long chunk = (long long)(scratch_cap_bytes() / std::max<size_t>(per_outer, 1));
     if (chunk < 1) chunk = 1;
     if (chunk > outer) chunk = outer;
-    const bool paired_epilogue = op.paired;
+    // realdft / DCT-2 / DST-2 over several passes: the last pass unpacks in
+    // mirror tiles when that kernel exists (the same choice run_pass makes);
+    // otherwise an unpack epilogue reads the packed spectrum back
+    bool mirror = false;
+    if (op.paired && np >= 2 && !strided && !lean_disabled()) {
+        const int lr = sch.plog[np - 1];
+        mirror = recorder() ? queue_has_lean(lr, 1, 1, LD_C, op.st)
+                            : (lr >= 4 && lean_available(lr, (lr <= 12 && lr <= 10) ? 8 : 9, 1, 1, LD_C, op.st));
+    }
+    const bool paired_epilogue = op.paired && !mirror;
     const int nbuf = paired_epilogue ? (np >= 2 ? 2 : 1) : (np >= 3 ? 2 : 1);
     // one resident launch per chunk for plain two-pass complex transforms of
     // contiguous lines

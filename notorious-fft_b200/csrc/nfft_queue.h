@@ -66,14 +66,19 @@ constexpr int QUEUE_LOG_TILE = 12;
     X(12, 0, 0, LD_C, ST_C)                                                                         \
     X(5, 1, 0, LD_C, ST_C) X(6, 1, 0, LD_C, ST_C) X(7, 1, 0, LD_C, ST_C) X(8, 1, 0, LD_C, ST_C)     \
     X(9, 1, 0, LD_C, ST_C) X(10, 1, 0, LD_C, ST_C)
-// Complex column/column passes; first passes of multi-pass realdft and DCT-2.
+// Complex column/column passes; first and last (mirror-tile unpack) passes of
+// multi-pass realdft and DCT-2.
 #define NFFT_QUEUE_LEAN_B(X)                                                                        \
     X(4, 1, 1, LD_C, ST_C) X(5, 1, 1, LD_C, ST_C) X(6, 1, 1, LD_C, ST_C) X(7, 1, 1, LD_C, ST_C)     \
     X(8, 1, 1, LD_C, ST_C) X(9, 1, 1, LD_C, ST_C) X(10, 1, 1, LD_C, ST_C)                           \
     X(5, 1, 0, LD_R2C, ST_C) X(6, 1, 0, LD_R2C, ST_C) X(7, 1, 0, LD_R2C, ST_C)                      \
     X(8, 1, 0, LD_R2C, ST_C) X(9, 1, 0, LD_R2C, ST_C) X(10, 1, 0, LD_R2C, ST_C)                     \
     X(5, 1, 0, LD_T2, ST_C) X(6, 1, 0, LD_T2, ST_C) X(7, 1, 0, LD_T2, ST_C)                         \
-    X(8, 1, 0, LD_T2, ST_C) X(9, 1, 0, LD_T2, ST_C) X(10, 1, 0, LD_T2, ST_C)
+    X(8, 1, 0, LD_T2, ST_C) X(9, 1, 0, LD_T2, ST_C) X(10, 1, 0, LD_T2, ST_C)                         \
+    X(4, 1, 1, LD_C, ST_R) X(5, 1, 1, LD_C, ST_R) X(6, 1, 1, LD_C, ST_R) X(7, 1, 1, LD_C, ST_R)     \
+    X(8, 1, 1, LD_C, ST_R) X(9, 1, 1, LD_C, ST_R) X(10, 1, 1, LD_C, ST_R)                           \
+    X(4, 1, 1, LD_C, ST_T2) X(5, 1, 1, LD_C, ST_T2) X(6, 1, 1, LD_C, ST_T2) X(7, 1, 1, LD_C, ST_T2) \
+    X(8, 1, 1, LD_C, ST_T2) X(9, 1, 1, LD_C, ST_T2) X(10, 1, 1, LD_C, ST_T2)
 // Single-pass realdft and DCT-2 / DST-2.
 #define NFFT_QUEUE_LEAN_C(X)                                                                        \
     X(4, 0, 0, LD_R2C, ST_R) X(5, 0, 0, LD_R2C, ST_R) X(6, 0, 0, LD_R2C, ST_R)                      \

@@ -387,10 +387,25 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
         const long long line0 = tile << Lt::LOGJ;
         if (line0 >= a.nlines) continue;
         for (auto& x : sm) x = mkc((T)NAN, (T)NAN);
+        const long long ns = 1ll << a.logNj, tpt = Lt::MIRROR ? (ns >> Lt::LOGJ) : 1;
+        const long long tt = Lt::MIRROR ? tile - (tile / tpt) * tpt : 0;
         for (int t = 0; t < Lt::J; ++t) {
             long long tmp[3];
             TileLines tl{&tmp[0], &tmp[1], &tmp[2]};
-            line_setup(a, line0 + t, 0, tl);
+            if constexpr (Lt::MIRROR) {
+                if (tpt < 1) {
+                    fprintf(stderr, "nfft_emu: mirror tile larger than the transform's lines\n");
+                    abort();
+                }
+                const long long jj = mirror_line(tt, t, Lt::J, ns);
+                if (jj < 0 || jj >= ns || mirror_local(tt, jj, Lt::J, ns) != t) {
+                    fprintf(stderr, "nfft_emu: mirror line map of tile %lld line %d is not invertible\n", tt, t);
+                    abort();
+                }
+                line_setup(a, (tile / tpt) * ns + jj, 0, tl);
+            } else {
+                line_setup(a, line0 + t, 0, tl);
+            }
             lines[t] = LeanLine{tmp[0], tmp[1], tmp[2]};
         }
         for (int t = 0; t < TH; ++t) {
@@ -421,7 +436,24 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
                                                      &regs[t * 16 + q * RHO]);
                 }
         }
-        if constexpr (Lt::PAIRED) {
+        if constexpr (Lt::MIRROR) {
+            const long long M = ns << LOGR;
+            constexpr int ITEMS = (Lt::J / 2) << LOGR;
+            for (int w = 0; w < ITEMS; ++w) {
+                const int l = w >> LOGR, r = w & ((1 << LOGR) - 1);
+                const LeanLine ln = lines[l];
+                const long long k = mirror_item_k(tt, l, r, 1 << LOGR, ns, ln.j);
+                unpack_pair<T, ST>(a, tw, ln.bout, k, M, [&](long long q) {
+                    const long long j = q & (ns - 1);
+                    const int ll = mirror_local(tt, j, Lt::J, ns);
+                    if (ll < 0 || ll >= Lt::J || lines[ll].j != j) {
+                        fprintf(stderr, "nfft_emu: mirror unpack reads line %lld outside its tile\n", j);
+                        abort();
+                    }
+                    return sm[NFFT_SM((lean_idx<true, LOGR, Lt::LOGJ>(ll, (int)(q >> a.logNj))))];
+                });
+            }
+        } else if constexpr (Lt::PAIRED) {
             constexpr int ITEMS = Lt::J << (LOGR - 1);
             for (int w = 0; w < ITEMS; ++w) {
                 int ll = w >> (LOGR - 1), k = w & ((1 << (LOGR - 1)) - 1);
