@@ -418,13 +418,14 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
     }
     if constexpr (L::MIRROR) {
         __syncthreads();
-        // mirror tile: (J/2 low lines) x R unpack items, each emitting bins k, M - k
+        // mirror tile: (J/2 low lines) x R unpack items, each emitting bins k, M - k;
+        // lines fastest, so neighbouring threads write neighbouring bins
         const long long ns = 1ll << a.logNj, tpt = ns >> L::LOGJ;
         const long long tt = tile - (tile / tpt) * tpt;
         const long long M = ns << LOGR;
         constexpr int ITEMS = (L::J / 2) << LOGR;
         for (int w = t; w < ITEMS; w += L::THREADS) {
-            const int l = w >> LOGR, r = w & ((1 << LOGR) - 1);
+            const int l = w & (L::J / 2 - 1), r = w >> (L::LOGJ - 1);
             const LeanLine ln = lines[l];
             const long long k = mirror_item_k(tt, l, r, 1 << LOGR, ns, ln.j);
             unpack_pair<T, STORE>(a, tw, ln.bout, k, M, [&](long long q) {

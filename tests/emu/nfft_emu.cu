@@ -440,7 +440,7 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
             const long long M = ns << LOGR;
             constexpr int ITEMS = (Lt::J / 2) << LOGR;
             for (int w = 0; w < ITEMS; ++w) {
-                const int l = w >> LOGR, r = w & ((1 << LOGR) - 1);
+                const int l = w & (Lt::J / 2 - 1), r = w >> (Lt::LOGJ - 1);
                 const LeanLine ln = lines[l];
                 const long long k = mirror_item_k(tt, l, r, 1 << LOGR, ns, ln.j);
                 unpack_pair<T, ST>(a, tw, ln.bout, k, M, [&](long long q) {
