@@ -137,7 +137,18 @@ FftSchedule make_schedule(int logL, bool strided, int max_tile) {
         s.plog[0] = logL;
         s.tile[0] = logL <= 12 ? 12 : 13;
     } else {
-        const int maxr = max_tile - jmin;
+        // largest pass radix: the tile must keep jmin lines.  Contiguous 2^19 and
+        // 2^20 axes run three passes of radix <= 2^8 instead of two of 2^10: the
+        // extra sweep costs less than the 64-byte rows of the big radices (B200:
+        // +3% / +16% FP64, +26% / +27% FP32).  NOTORIOUS_FFT_MAX_PASS_LOG sets
+        // the cap for every size.
+        static const int cap_env = [] {
+            const char* e = getenv("NOTORIOUS_FFT_MAX_PASS_LOG");
+            return e ? atoi(e) : 0;
+        }();
+        const int cap = cap_env ? cap_env : ((!strided && logL >= 19 && logL <= 20 && max_tile == 13) ? 8 : 0);
+        int maxr = max_tile - jmin;
+        if (cap >= 4 && cap < maxr) maxr = cap;
         int np = (logL + maxr - 1) / maxr;
         if (np < 1) np = 1;
         s.npass = np;
@@ -285,20 +296,19 @@ static void set_lines(PassArgs& a, const View& src, const View& dst, long long n
     a.nlines = n;
 }
 
-// Two-pass complex transforms of 2^logL points: one resident launch per chunk
-// (both passes, scratch in L2) or two launches.  The resident form halves the
-// DRAM traffic but is bound by the SMs' tile throughput, which the two
-// launches already nearly saturate at ~90% of HBM bandwidth; on B200 it wins
-// only for FP64 at 2^19 points.  NOTORIOUS_FFT_RESIDENT=1 / 0 forces it on /
-// off for every size.
+// Two-pass complex transforms: one resident launch per chunk (both passes,
+// scratch in L2) when NOTORIOUS_FFT_RESIDENT=1, else two launches.  The
+// resident form halves the DRAM traffic but is bound by the SMs' tile
+// throughput, which the two launches already nearly saturate at ~90% of HBM
+// bandwidth; on B200 it is not faster than the default schedules at any size.
 static bool resident_enabled(int logL) {
     static int v = -2;
     if (v == -2) {
         const char* e = getenv("NOTORIOUS_FFT_RESIDENT");
-        v = e ? (atoi(e) != 0 ? 1 : 0) : -1;
+        v = e ? (atoi(e) != 0 ? 1 : 0) : 0;
     }
-    if (v >= 0) return v == 1;
-    return sizeof(real_t) == 8 && logL == 19;
+    (void)logL;
+    return v == 1;
 }
 
 // L2 policy: NOTORIOUS_FFT_CACHE_HINTS=0 turns the hints off.
@@ -316,11 +326,15 @@ static int env_int(const char* name, int dflt) {
     return e ? atoi(e) : dflt;
 }
 // Tuning knobs (defaults chosen from measurements on B200):
-//   NOTORIOUS_FFT_LEAN_LOGT  threads (log2) of the complex pass kernels
+//   NOTORIOUS_FFT_LEAN_LOGT  threads (log2) of the complex pass kernels: 128
+//       (2048-point tiles) by default, 256 for the radix-2^9 passes of 2^17 /
+//       2^18 axes (and 2^16 in float), where 4096-point tiles keep 128-byte
+//       rows (B200: +7% / +19% FP64, +5..31% FP32)
 //   NOTORIOUS_FFT_TW_MODE    pre-twiddle generation (0 tree, 1 chains, 2 tables)
-static int lean_logt_pref() {
-    static int v = env_int("NOTORIOUS_FFT_LEAN_LOGT", 7);
-    return v;
+static int lean_logt_pref(int logL) {
+    static int v = env_int("NOTORIOUS_FFT_LEAN_LOGT", 0);
+    if (v) return v;
+    return (logL == 17 || logL == 18 || (sizeof(real_t) == 4 && logL == 16)) ? 8 : 7;
 }
 static int tw_mode() {
     static int v = env_int("NOTORIOUS_FFT_TW_MODE", 1);
@@ -423,7 +437,7 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
         const int ci = a.in_row ? 0 : 1, co = a.out_row ? 0 : 1;
         const bool rr = !ci && !co;
         int logT = (logR <= 12 && (rr || logR <= 10)) ? 8 : 9;
-        if (lean_logt_pref() == 7 && lean_available(logR, 7, ci, co, ldop, stop)) logT = 7;
+        if (lean_logt_pref(logL) == 7 && lean_available(logR, 7, ci, co, ldop, stop)) logT = 7;
         if (lean_available(logR, logT, ci, co, ldop, stop)) {
             a.logJ = logT + 4 - logR;
             long long nt = (a.nlines + (1ll << a.logJ) - 1) >> a.logJ;
