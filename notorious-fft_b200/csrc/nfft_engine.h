@@ -83,7 +83,8 @@ struct FftSchedule {
 };
 // strided: the axis is not contiguous (every pass runs in column mode).
 // max_tile: log2 of the largest tile (13: 512-thread kernels; 12: the queue).
-FftSchedule make_schedule(int logL, bool strided, int max_tile = 13);
+// max_pass_log: largest pass radix (log2); -1 = the default rule, 0 = no cap.
+FftSchedule make_schedule(int logL, bool strided, int max_tile = 13, int max_pass_log = -1);
 // Explicit pass radices (log2, execution order; 4096-point tiles).  False when
 // the split is not executable (radix too large for its tile, wrong sum).
 bool make_split_schedule(int logL, const int* plog, int npass, FftSchedule* out);

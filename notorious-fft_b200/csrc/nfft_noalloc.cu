@@ -102,16 +102,23 @@ extern "C" int notorious_fft_dft_noalloc(const notorious_fft_cmpl* x, notorious_
     cudaStream_t s = (cudaStream_t)stream;
     int logN = 0;
     while ((1 << logN) < N) ++logN;
-    const FftSchedule sch = make_schedule(logN, false);
-    OpSpec op;
-    op.conj_in = op.conj_out = inverse ? 1 : 0;
     const long long L = N;
-    // whole transforms per scratch fill
-    const long long chunk = sch.npass == 1 ? howmany : std::max<long long>(1, NOALLOC_SCRATCH_ELEMS / L);
-    if (sch.npass > 2) {
+    const long long half = NOALLOC_SCRATCH_ELEMS / 2;
+    // The default schedule, unless it runs more than two passes (the passes
+    // then alternate between the two halves of the scratch array) and a
+    // transform does not fit in half: then the uncapped two-pass schedule.
+    FftSchedule sch = make_schedule(logN, false);
+    if (sch.npass > 2 && L > half) sch = make_schedule(logN, false, 13, 0);
+    if (sch.npass > 2 && L > half) {
         set_error(NOTORIOUS_FFT_ERR_UNSUPPORTED, "schedule needs more than one scratch buffer");
         return NOTORIOUS_FFT_ERR_UNSUPPORTED;
     }
+    OpSpec op;
+    op.conj_in = op.conj_out = inverse ? 1 : 0;
+    // whole transforms per scratch fill
+    const long long per_buf = sch.npass > 2 ? half : NOALLOC_SCRATCH_ELEMS;
+    const long long chunk = sch.npass == 1 ? howmany : std::max<long long>(1, per_buf / L);
+    cplx_t* const bufs[2] = {d->scratch, d->scratch + half};
     for (long long b0 = 0; b0 < howmany; b0 += chunk) {
         const long long cn = std::min(chunk, (long long)howmany - b0);
         View vs, vd;
@@ -123,19 +130,17 @@ extern "C" int notorious_fft_dft_noalloc(const notorious_fft_cmpl* x, notorious_
             vs.cnt[0] = vd.cnt[0] = cn;
             vs.str[0] = vd.str[0] = L;
         }
-        if (sch.npass == 1) {
-            if (!run_pass(&ctx, vs, vd, logN, 0, sch.plog[0], sch.tile[0], sch.nsub[0], sch.sub[0], op, true, true, 0, 0,
-                          nullptr, nullptr, s))
+        View cur = vs;
+        int logNs = 0;
+        for (int i = 0; i < sch.npass; ++i) {
+            const bool first = i == 0, last = i == sch.npass - 1;
+            const View out = last ? vd : scratch_view(sch.npass > 2 ? bufs[i & 1] : d->scratch, vs, L, false);
+            if (!run_pass(&ctx, cur, out, logN, logNs, sch.plog[i], sch.tile[i], sch.nsub[i], sch.sub[i], op, first,
+                          last, 0, logNs, nullptr, nullptr, s, !first, !last))
                 return last_error() ? last_error() : NOTORIOUS_FFT_ERR_CUDA;
-            continue;
+            logNs += sch.plog[i];
+            cur = out;
         }
-        View mid = scratch_view(d->scratch, vs, L, false);
-        if (!run_pass(&ctx, vs, mid, logN, 0, sch.plog[0], sch.tile[0], sch.nsub[0], sch.sub[0], op, true, false, 0, 0,
-                      nullptr, nullptr, s, false, true))
-            return last_error() ? last_error() : NOTORIOUS_FFT_ERR_CUDA;
-        if (!run_pass(&ctx, mid, vd, logN, sch.plog[0], sch.plog[1], sch.tile[1], sch.nsub[1], sch.sub[1], op, false,
-                      true, 0, sch.plog[0], nullptr, nullptr, s, true, false))
-            return last_error() ? last_error() : NOTORIOUS_FFT_ERR_CUDA;
     }
     return 0;
 }

@@ -128,7 +128,7 @@ static void split_sub(int logR, int* nsub, int* sub) {
     *nsub = n;
 }
 
-FftSchedule make_schedule(int logL, bool strided, int max_tile) {
+FftSchedule make_schedule(int logL, bool strided, int max_tile, int max_pass_log) {
     FftSchedule s;
     s.logL = logL;
     const int jmin = log_jmin();
@@ -137,18 +137,21 @@ FftSchedule make_schedule(int logL, bool strided, int max_tile) {
         s.plog[0] = logL;
         s.tile[0] = logL <= 12 ? 12 : 13;
     } else {
-        // largest pass radix: the tile must keep jmin lines.  Contiguous 2^19 and
-        // 2^20 axes run three passes of radix <= 2^8 instead of two of 2^10: the
-        // extra sweep costs less than the 64-byte rows of the big radices (B200:
-        // +3% / +16% FP64, +26% / +27% FP32).  NOTORIOUS_FFT_MAX_PASS_LOG sets
+        // largest pass radix: the tile must keep jmin lines.  Contiguous axes of
+        // 2^19..2^24 points run passes of radix <= 2^8 (three instead of two
+        // for 2^19..2^22): the extra sweep costs less than the 64-byte rows of
+        // the big radices (B200, 1 GiB batches: FP64 +13% / +15% / +30% / +37%
+        // at 2^19 / 2^20 / 2^21 / 2^22, FP32 +26% / +27% at 2^19 / 2^20 and
+        // the same schedule as before above).  NOTORIOUS_FFT_MAX_PASS_LOG sets
         // the cap for every size.
         static const int cap_env = [] {
             const char* e = getenv("NOTORIOUS_FFT_MAX_PASS_LOG");
             return e ? atoi(e) : 0;
         }();
-        const int cap = cap_env ? cap_env : ((!strided && logL >= 19 && logL <= 20 && max_tile == 13) ? 8 : 0);
+        const int cap = max_pass_log >= 0 ? max_pass_log
+                        : cap_env ? cap_env : ((!strided && logL >= 19 && logL <= 24 && max_tile == 13) ? 8 : 0);
         int maxr = max_tile - jmin;
-        if (cap >= 4 && cap < maxr) maxr = cap;
+        if (cap >= 4 && cap < maxr) maxr = std::max(cap, (logL + 3) / 4);   // at most 4 passes
         int np = (logL + maxr - 1) / maxr;
         if (np < 1) np = 1;
         s.npass = np;
