@@ -225,6 +225,13 @@ struct ResidentEntry {
     size_t smem_pf;
 };
 const ResidentEntry* resident_find(int r1, int r2);
+// Resident kernels fed by tensor copies: NG consumer groups, S stage buffers.
+struct ResidentTmaEntry {
+    int r1, r2, logt, ng, stages;
+    const void* fn;
+    size_t smem;
+};
+const ResidentTmaEntry* resident_tma_find(int r1, int r2);
 bool resident_set_attributes();
 bool launch_resident(const DeviceCtx* c, const PassArgs& a1, const PassArgs& a2, int r1, int r2, long long B,
                      unsigned* ctr, cudaStream_t s);

@@ -117,6 +117,7 @@ struct Lean {
     static constexpr int J = 1 << LOGJ;
     static constexpr int R = 1 << LOGR;
     static constexpr int LOGR_ = LOGR;
+    static constexpr bool COL_OUT_ = COL_OUT;
     static constexpr bool PAIRED = (STORE == ST_R || STORE == ST_T2);
     // shared layout: column tiles whenever either side walks lines
     static constexpr bool COLL = COL_IN || COL_OUT;

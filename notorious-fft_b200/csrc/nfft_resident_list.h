@@ -11,3 +11,11 @@
 #define NFFT_RESIDENT_A(X) X(7, 6, 7) X(7, 7, 7) X(8, 7, 7) X(8, 8, 7)
 #define NFFT_RESIDENT_B(X) X(9, 8, 7) X(9, 9, 7) X(10, 9, 8) X(10, 10, 8)
 #endif
+
+// Resident kernels fed by tensor copies (nfft_resident_tma.cuh):
+// X(LOGR1, LOGR2, LOGT, NG) with NG consumer groups of 2^LOGT threads per CTA.
+#if defined(NFFT_REAL_IS_FLOAT) && NFFT_REAL_IS_FLOAT
+#define NFFT_RESIDENT_TMA(X) X(7, 6, 7, 6) X(7, 7, 7, 6) X(8, 7, 7, 6) X(8, 8, 7, 6)
+#else
+#define NFFT_RESIDENT_TMA(X) X(7, 6, 7, 3) X(7, 7, 7, 3) X(8, 7, 7, 3) X(8, 8, 7, 3)
+#endif

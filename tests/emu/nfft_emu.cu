@@ -40,7 +40,8 @@ static bool inside(const std::map<uintptr_t, size_t>& m, uintptr_t p, size_t b) 
 }
 
 cudaError_t Malloc(void** p, size_t bytes) {
-    void* q = malloc(bytes ? bytes : 1);
+    // 256-byte aligned, like cudaMalloc (tensor copies and L2 discards rely on it)
+    void* q = aligned_alloc(256, (bytes + 255) / 256 * 256 + (bytes ? 0 : 256));
     if (!q) return cudaErrorMemoryAllocation;
     // NaN fill: scratch read before it is written poisons the result
     double nan = NAN;
@@ -200,6 +201,7 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 #include "../../notorious-fft_b200/csrc/nfft_queue.h"
 #include "../../notorious-fft_b200/csrc/nfft_resident.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_resident_list.h"
+#include "../../notorious-fft_b200/csrc/nfft_resident_tma.cuh"
 
 // ---------------------------------------------------------------------------
 // emulated launches: the kernels' phase functions for every thread
@@ -760,6 +762,158 @@ const ResidentEntry* resident_find(int r1, int r2) {
 }
 bool resident_set_attributes() { return true; }
 static long long g_resident_launches = 0;
+
+// ---- resident kernels fed by tensor copies: the same work order; every tile
+// is staged the way the kernel stages it -- the tensor copy restated on the
+// CPU from the host's box geometry (tma_pass_geom / tma_tile_coords, every
+// source element bounds-checked, the inner coordinate's 16-byte rule
+// asserted) into a NaN-filled stage buffer -- and computed by the consumer
+// group's phases with the exchanges in place in that buffer.
+static std::vector<ResidentTmaEntry>& emu_resident_tma_registry() {
+    static std::vector<ResidentTmaEntry> v = [] {
+        std::vector<ResidentTmaEntry> r;
+#define X(R1, R2, LT, NG) \
+    r.push_back(ResidentTmaEntry{R1, R2, LT, NG, TmaRes<real_t, R1, R2, LT>::stages(NG), nullptr, \
+                                 TmaRes<real_t, R1, R2, LT>::smem_bytes(NG)});
+        NFFT_RESIDENT_TMA(X)
+#undef X
+        return r;
+    }();
+    return v;
+}
+const ResidentTmaEntry* resident_tma_find(int r1, int r2) {
+    for (auto& e : emu_resident_tma_registry())
+        if (e.r1 == r1 && e.r2 == r2) return &e;
+    return nullptr;
+}
+
+template <typename Lt, size_t STAGE, size_t TILE_BYTES>
+static void emu_tma_tile(const PassArgs& a, long long gt, long long B) {
+    using T = real_t;
+    using V = C2<T>;
+    const TwTables<T>* tw = (const TwTables<T>*)a.tw;
+    constexpr int TH = Lt::THREADS;
+    constexpr int LOGR = Lt::LOGR_;
+    static_assert(STAGE >= TILE_BYTES && STAGE >= sizeof(V) * (size_t)Lt::SMEM_ELEMS, "stage too small");
+    std::vector<V> st(STAGE / sizeof(V), mkc((T)NAN, (T)NAN));
+    g_smem_elems = (int)(STAGE / sizeof(V));
+    // the tensor copy
+    const long long bstride = a.ndims > 1 ? a.istr[1] : (1ll << (a.logNj + LOGR));
+    const TmaPassGeom g = tma_pass_geom(a.logNj, LOGR, Lt::LOGJ, B, bstride, sizeof(V));
+    int x, z;
+    tma_tile_coords(gt, Lt::LOGJ, a.logNj, x, z);
+    if ((size_t)g.box[0] * g.box[1] * g.nbox * sizeof(T) != TILE_BYTES || (x * sizeof(T)) % 16 ||
+        (g.box[0] * sizeof(T)) % 16 || x + g.box[0] > g.dim[0] || (unsigned long long)z >= g.dim[2] ||
+        g.stride_bytes[0] % 16 || g.stride_bytes[1] % 16 || a.in_estride != 1) {
+        fprintf(stderr, "nfft_emu: tensor copy of tile %lld breaks the box rules (x %d z %d)\n", gt, x, z);
+        abort();
+    }
+    T* sr = (T*)st.data();
+    for (int k = 0; k < g.nbox; ++k)
+        for (unsigned yy = 0; yy < g.box[1]; ++yy)
+            for (unsigned xx = 0; xx < g.box[0]; ++xx) {
+                const unsigned long long y = (unsigned long long)k * g.box[1] + yy;
+                const T* src = (const T*)((const unsigned char*)a.in + (unsigned long long)z * g.stride_bytes[1] +
+                                          y * g.stride_bytes[0]) + x + xx;
+                nfft_emu_check(src, sizeof(T), 0);
+                sr[y * g.box[0] + xx] = *src;
+            }
+    // consumer phases
+    std::vector<LeanLine> lines(Lt::J);
+    for (int t = 0; t < Lt::J; ++t) {
+        long long bin, bout, j;
+        int i_;
+        resident_line(a, Lt::LOGJ, LOGR, gt, t, bin, bout, j, i_);
+        lines[t] = LeanLine{bin, bout, j};
+    }
+    if (a.discard_in)
+        for (int w = 0; w < ((Lt::J * (int)sizeof(V) / 128) << LOGR); ++w) {
+            const void* p = tma_discard_line<Lt, V>(a, gt, w);
+            if (p && ((uintptr_t)p & 127)) {
+                fprintf(stderr, "nfft_emu: discarded scratch line is not 128-byte aligned\n");
+                abort();
+            }
+            if (p) nfft_emu_check(p, 128, 0);
+        }
+    std::vector<V> regs((size_t)TH * 16);
+    std::vector<int> ls((size_t)TH * 16), is((size_t)TH * 16);
+    for (int t = 0; t < TH; ++t) tma_stage_read<Lt, V>(a, st.data(), t, &regs[t * 16], ls[t * 16], is[t * 16]);
+    for (int t = 0; t < TH; ++t) {
+        const int l = ls[t * 16], i = is[t * 16];
+        const long long j = ((gt << Lt::LOGJ) + l) & ((1ll << a.logNj) - 1);
+        Lt::pre_twiddle_dft(a, tw, j, i, &regs[t * 16]);
+        Lt::template write_smem<0>(st.data(), l, i, &regs[t * 16]);
+    }
+    auto middle = [&](auto Sc) {
+        constexpr int S = decltype(Sc)::value;
+        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+        for (int t = 0; t < TH; ++t)
+            for (int q = 0; q < 16 / RHO; ++q)
+                Lt::template read<S, Lt::COLL>(st.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
+        for (int t = 0; t < TH; ++t)
+            for (int q = 0; q < 16 / RHO; ++q) {
+                Lt::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
+                Lt::template write_smem<S>(st.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
+            }
+    };
+    if constexpr (Lt::NS >= 3) middle(std::integral_constant<int, 1>{});
+    if constexpr (Lt::NS >= 4) middle(std::integral_constant<int, 2>{});
+    constexpr int S = Lt::NS - 1;
+    constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+    for (int t = 0; t < TH; ++t)
+        for (int q = 0; q < 16 / RHO; ++q)
+            Lt::template read<S, Lt::COL_OUT_>(st.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
+    for (int t = 0; t < TH; ++t)
+        for (int q = 0; q < 16 / RHO; ++q) {
+            Lt::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
+            Lt::template write_global<S>(a, tw, lines.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
+        }
+}
+
+typedef void (*EmuTmaTile)(const PassArgs&, long long, long long);
+static long long g_resident_tma_launches = 0;
+
+static bool emu_resident_tma(const ResidentTmaEntry* e, const PassArgs& a1, const PassArgs& a2, long long B) {
+    static std::map<std::pair<int, int>, std::pair<EmuTmaTile, EmuTmaTile>> fns = [] {
+        std::map<std::pair<int, int>, std::pair<EmuTmaTile, EmuTmaTile>> m;
+#define X(R1, R2, LT, NG)                                                                                         \
+    m[{R1, R2}] = {emu_tma_tile<TmaRes<real_t, R1, R2, LT>::L1, TmaRes<real_t, R1, R2, LT>::STAGE,                \
+                                TmaRes<real_t, R1, R2, LT>::TILE_BYTES>,                                          \
+                   emu_tma_tile<TmaRes<real_t, R1, R2, LT>::L2, TmaRes<real_t, R1, R2, LT>::STAGE,                \
+                                TmaRes<real_t, R1, R2, LT>::TILE_BYTES>};
+        NFFT_RESIDENT_TMA(X)
+#undef X
+        return m;
+    }();
+    if (e->stages <= e->ng || e->smem > 232448) {
+        fprintf(stderr, "nfft_emu: tensor-copy resident kernel %d x %d: %d stages for %d groups, %zu bytes\n", e->r1,
+                e->r2, e->stages, e->ng, e->smem);
+        abort();
+    }
+    const auto& f = fns[{e->r1, e->r2}];
+    const int lt = e->r1 + e->r2 - (e->logt + 4);
+    const long long T = 1ll << lt, lag = std::min<long long>(B, 2);
+    std::vector<long long> done((size_t)B, 0);
+    g_launches++;
+    g_resident_launches++;
+    g_resident_tma_launches++;
+    for (long long g = 0; g < 2 * B * T; ++g) {
+        int pass;
+        long long tr, tile;
+        resident_decode(g, B, lag, lt, pass, tr, tile);
+        if (pass == 2 && done[tr] != T) {
+            fprintf(stderr, "nfft_emu: resident pass-2 item %lld before its pass 1\n", g);
+            abort();
+        }
+        if (pass == 1) {
+            f.first(a1, (tr << lt) + tile, B);
+            done[tr]++;
+        } else {
+            f.second(a2, (tr << lt) + tile, B);
+        }
+    }
+    return true;
+}
 bool launch_resident(const DeviceCtx*, const PassArgs& a1, const PassArgs& a2, int r1, int r2, long long B,
                      unsigned*, cudaStream_t) {
     static std::map<std::pair<int, int>, std::pair<EmuLean, EmuLean>> fns = [] {
@@ -770,6 +924,9 @@ bool launch_resident(const DeviceCtx*, const PassArgs& a1, const PassArgs& a2, i
 #undef X
         return m;
     }();
+    static const int mode = getenv("NOTORIOUS_FFT_RESIDENT") ? atoi(getenv("NOTORIOUS_FFT_RESIDENT")) : 0;
+    if (mode == 2)
+        if (const ResidentTmaEntry* te = resident_tma_find(r1, r2)) return emu_resident_tma(te, a1, a2, B);
     const ResidentEntry* e = resident_find(r1, r2);
     if (!e) {
         set_error(6, "no resident kernel for radices 2^%d x 2^%d", r1, r2);
@@ -921,4 +1078,5 @@ long long nfft_emu_cluster_launches(void) { return nfft::g_cluster_launches; }
 long long nfft_emu_checks(void) { return emu::n_checks; }
 long long nfft_emu_queue_items(void) { return nfft::g_queue_items; }
 long long nfft_emu_resident_launches(void) { return nfft::g_resident_launches; }
+long long nfft_emu_resident_tma_launches(void) { return nfft::g_resident_tma_launches; }
 }
