@@ -39,7 +39,7 @@ METRIC = "HBM GB/s, % roofline: FP64 drop-in vs batched split-TC form at stated 
 # DRAM bytes per transform (dram__bytes_read.sum + dram__bytes_write.sum over
 # both pass kernels) from an ncu capture of 256 transforms of the same shape;
 # scaled to the batch for roofline.traffic.
-MEASURED_TRAFFIC_PER_TRANSFORM = {("c2c", 65536): 3.64e6}
+MEASURED_TRAFFIC_PER_TRANSFORM = {("c2c", 65536): 3.82e6}
 
 WORKLOADS = {
     "c2c": dict(N=65536, batch=4096, l2="inputs 4 GiB per array > L2 (no flush)", flush=False),
