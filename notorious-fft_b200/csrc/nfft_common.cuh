@@ -98,6 +98,31 @@ NFFT_HD void gstore(float2* p, float2 v, int hint) {
 #endif
 }
 
+// Load of a table every transform of a batch reads again (Bluestein chirp and
+// filter spectrum): kept in L2 with evict_last priority.
+NFFT_HD double2 gload_keep(const double2* p) {
+#if defined(__CUDA_ARCH__)
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    double2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+    return v;
+#else
+    return NFFT_GLD(p);
+#endif
+}
+NFFT_HD float2 gload_keep(const float2* p) {
+#if defined(__CUDA_ARCH__)
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    float2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+    return v;
+#else
+    return NFFT_GLD(p);
+#endif
+}
+
 // Drop a 128-byte line from L2 without writing it back (dead scratch data).
 NFFT_HD void discard_l2(const void* p) {
 #if defined(__CUDA_ARCH__)

@@ -107,7 +107,7 @@ NFFT_HD C2<T> load_elem(const PassArgs& a, const TwTables<T>* tw, long long base
         if (p >= a.N) return mkc((T)0, (T)0);
         V v = NFFT_GLD(&((const V*)a.in)[base + p * a.in_estride]);
         if (a.conj_in) v.y = -v.y;
-        return cmul(v, NFFT_GLD(&((const V*)a.chirp)[p]));
+        return cmul(v, gload_keep(&((const V*)a.chirp)[p]));
     } else if constexpr (OP == LD_BLUE_R || OP == LD_BLUE_T2) {
         if (p >= a.N) return mkc((T)0, (T)0);
         const T* x = (const T*)a.in + base;
@@ -115,10 +115,10 @@ NFFT_HD C2<T> load_elem(const PassArgs& a, const TwTables<T>* tw, long long base
         T r;
         if constexpr (OP == LD_BLUE_R) r = NFFT_GLD(&x[p * es]);
         else r = (p < (a.N + 1) / 2) ? NFFT_GLD(&x[(2 * p) * es]) : NFFT_GLD(&x[(2 * a.N - 1 - 2 * p) * es]);
-        return cscale(NFFT_GLD(&((const V*)a.chirp)[p]), r);
+        return cscale(gload_keep(&((const V*)a.chirp)[p]), r);
     } else if constexpr (OP == LD_FILT) {
         const V v = NFFT_GLD(&((const V*)a.in)[base + p * a.in_estride]);
-        return cconj(cmul(v, NFFT_GLD(&((const V*)a.filt)[p])));
+        return cconj(cmul(v, gload_keep(&((const V*)a.filt)[p])));
     } else if constexpr (OP == LD_R2C) {
         const T* x = (const T*)a.in + base;
         const long long es = a.in_estride;
@@ -209,18 +209,18 @@ NFFT_HD void store_elem(const PassArgs& a, const TwTables<T>* tw, long long base
     } else if constexpr (OP == ST_BLUE) {
         if (q >= a.N) return;
         v = cconj(v);                                  // leave the conjugated inverse-FFT domain
-        v = cmul(v, NFFT_GLD(&((const V*)a.chirp)[q]));
+        v = cmul(v, gload_keep(&((const V*)a.chirp)[q]));
         if (a.conj_out) v.y = -v.y;
         if (a.scale != 1.0) v = cscale(v, (T)a.scale);
         NFFT_GST(&((V*)a.out)[base + q * a.out_estride], v);
     } else if constexpr (OP == ST_BLUE_R) {
         if (q > a.N / 2) return;
-        v = cmul(cconj(v), NFFT_GLD(&((const V*)a.chirp)[q]));
+        v = cmul(cconj(v), gload_keep(&((const V*)a.chirp)[q]));
         if (a.scale != 1.0) v = cscale(v, (T)a.scale);
         NFFT_GST(&((V*)a.out)[base + q * a.out_estride], v);
     } else if constexpr (OP == ST_BLUE_T2) {
         if (q >= a.N) return;
-        v = cmul(cconj(v), NFFT_GLD(&((const V*)a.chirp)[q]));
+        v = cmul(cconj(v), gload_keep(&((const V*)a.chirp)[q]));
         const V w = NFFT_GLD(&((const V*)a.post)[q]);
         T y = (T)2 * (v.x * w.x - v.y * w.y);
         if (a.scale != 1.0) y = (T)(y * a.scale);
@@ -269,9 +269,10 @@ NFFT_HD C2<T> real_unpack(C2<T> a, C2<T> b, C2<T> w) {
 }
 
 // Emit realdft bin k (0 <= k <= M) as ST_R (complex bin) or ST_T2 (DCT-2 /
-// DST-2 outputs derived from the bin).
+// DST-2 outputs derived from the bin; t = e^{-i pi k / 2N} for 0 < k < M).
 template <typename T, int OP>
-NFFT_HD void emit_bin(const PassArgs& a, const TwTables<T>* tw, long long base, long long k, C2<T> X) {
+NFFT_HD void emit_bin(const PassArgs& a, const TwTables<T>* tw, long long base, long long k, C2<T> X,
+                      C2<T> t = C2<T>{}) {
     using V = C2<T>;
     const long long N = a.N, M = N / 2;
     if constexpr (OP == ST_R) {
@@ -287,7 +288,7 @@ NFFT_HD void emit_bin(const PassArgs& a, const TwTables<T>* tw, long long base, 
         } else if (k == M) {
             NFFT_GST(&y[(a.dst ? M - 1 : M) * es], (T)2 * K<T>::r2 * X.x);
         } else {
-            V t = twiddle<T>(tw, (uint64_t)k, a.logN + 2);     // e^{-i pi k / 2N}
+            (void)tw;
             T c = (T)2 * (X.x * t.x - X.y * t.y);
             T s = (T)-2 * (X.x * t.y + X.y * t.x);
             if (!a.dst) { NFFT_GST(&y[k * es], c); NFFT_GST(&y[(N - k) * es], s); }
@@ -308,12 +309,22 @@ NFFT_HD void unpack_pair(const PassArgs& a, const TwTables<T>* tw, long long bas
         emit_bin<T, OP>(a, tw, base, M, mkc(z0.x - z0.y, (T)0));
         if (M >= 2) {
             V zh = zget(M / 2);
-            emit_bin<T, OP>(a, tw, base, M / 2, mkc(zh.x, -zh.y));
+            // bin M/2 = N/4: post-twiddle e^{-i pi / 8}
+            emit_bin<T, OP>(a, tw, base, M / 2, mkc(zh.x, -zh.y), mkc(K<T>::c8, -K<T>::s8));
         }
     } else {
         V zk = zget(k), zm = zget(M - k);
-        emit_bin<T, OP>(a, tw, base, k, real_unpack<T>(zk, zm, twiddle<T>(tw, (uint64_t)k, a.logN)));
-        emit_bin<T, OP>(a, tw, base, M - k, real_unpack<T>(zm, zk, twiddle<T>(tw, (uint64_t)(M - k), a.logN)));
+        // W_N^{M-k} = -conj(W_N^k) exactly (W_N^M = -1): one table twiddle per pair
+        const V w = twiddle<T>(tw, (uint64_t)k, a.logN);
+        const V wm = mkc(-w.x, w.y);
+        V t = V{}, tm = V{};
+        if constexpr (OP == ST_T2) {
+            // e^{-i pi (M-k) / 2N} = e^{-i pi / 4} conj(e^{-i pi k / 2N})
+            t = twiddle<T>(tw, (uint64_t)k, a.logN + 2);
+            tm = mkc((t.x - t.y) * K<T>::r2, -(t.x + t.y) * K<T>::r2);
+        }
+        emit_bin<T, OP>(a, tw, base, k, real_unpack<T>(zk, zm, w), t);
+        emit_bin<T, OP>(a, tw, base, M - k, real_unpack<T>(zm, zk, wm), tm);
     }
 }
 
@@ -445,7 +456,7 @@ NFFT_HD void mid_slot(const PassArgs& a, C2<T>* sm, TileLines tl, int e) {
     if (j < 0) return;
     long long q = ((j >> logNs) << (logNs + logR)) + (j & ((1ll << logNs) - 1)) + ((long long)r << logNs);
     C2<T> v = sm[NFFT_SM(spad(e))];
-    sm[NFFT_SM(spad(e))] = cconj(cmul(v, NFFT_GLD(&((const C2<T>*)a.filt)[q])));
+    sm[NFFT_SM(spad(e))] = cconj(cmul(v, gload_keep(&((const C2<T>*)a.filt)[q])));
 }
 
 // Store tile slot e with an element-wise output operator.
