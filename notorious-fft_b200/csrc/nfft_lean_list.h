@@ -64,4 +64,14 @@
     X(7, 8, 1, 1, LD_C, ST_BLUE) X(8, 8, 1, 1, LD_C, ST_BLUE) X(9, 8, 1, 1, LD_C, ST_BLUE)         \
     X(10, 8, 1, 1, LD_C, ST_BLUE) X(11, 9, 1, 1, LD_C, ST_BLUE)
 
-#define NFFT_LEAN_ALL(X) NFFT_LEAN_C2C(X) NFFT_LEAN_REAL(X) NFFT_LEAN_MULTI(X) NFFT_LEAN_C2C_T7(X) NFFT_LEAN_BLUE(X)
+// the fused operators of multi-pass real and Bluestein transforms on 2048-point
+// tiles for the radices whose column tiles keep >= 8 lines (the planner takes
+// them where it prefers 128-thread tiles, as for the complex passes)
+#define NFFT_LEAN_OPS_T7_ONE(X, R)                                                                 \
+    NFFT_LEAN_MULTI_ONE(X, R, 7)                                                                   \
+    X(R, 7, 1, 0, LD_BLUE, ST_C) X(R, 7, 1, 0, LD_FILT, ST_C) X(R, 7, 1, 1, LD_C, ST_BLUE)
+#define NFFT_LEAN_OPS_T7(X) NFFT_LEAN_OPS_T7_ONE(X, 6) NFFT_LEAN_OPS_T7_ONE(X, 7) NFFT_LEAN_OPS_T7_ONE(X, 8)
+
+#define NFFT_LEAN_ALL(X)                                                                           \
+    NFFT_LEAN_C2C(X) NFFT_LEAN_REAL(X) NFFT_LEAN_MULTI(X) NFFT_LEAN_C2C_T7(X) NFFT_LEAN_BLUE(X)     \
+    NFFT_LEAN_OPS_T7(X)
