@@ -466,10 +466,14 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
 #ifndef NFFT_LEAN_MINB_T8_F32
 #define NFFT_LEAN_MINB_T8_F32 4
 #endif
+#ifndef NFFT_LEAN_MINB_T9_F32
+#define NFFT_LEAN_MINB_T9_F32 2
+#endif
 template <typename T, int LOGT>
 constexpr int lean_min_blocks() {
     return LOGT <= 7 ? (sizeof(T) == 4 ? NFFT_LEAN_MINB_T7_F32 : NFFT_LEAN_MINB_T7_F64)
-                     : (LOGT == 8 ? (sizeof(T) == 4 ? NFFT_LEAN_MINB_T8_F32 : NFFT_LEAN_MINB_T8_F64) : 1);
+                     : (LOGT == 8 ? (sizeof(T) == 4 ? NFFT_LEAN_MINB_T8_F32 : NFFT_LEAN_MINB_T8_F64)
+                                  : (sizeof(T) == 4 ? NFFT_LEAN_MINB_T9_F32 : 1));
 }
 
 template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
