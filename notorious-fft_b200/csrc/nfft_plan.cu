@@ -423,11 +423,14 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
     }
     if (Recorder* rec = recorder()) {
         // queue form: a branch of the persistent 256-thread kernel.  Scratch
-        // written earlier in the same launch is read through L2 (hint 3).
+        // written earlier in the same launch is read through L2 (hint 3, for
+        // coherence); NOTORIOUS_FFT_QUEUE_KEEP=0 drops the keep-in-L2 policy
+        // (evict_last scratch stores, discard after the read).
+        static const int keep = env_int("NOTORIOUS_FFT_QUEUE_KEEP", 1);
         if (in_scratch || out_scratch) {
             a.hint_in = in_scratch ? 3 : 1;
-            a.hint_out = out_scratch ? 2 : 1;
-            a.discard_in = in_scratch ? 1 : 0;
+            a.hint_out = out_scratch ? (keep ? 2 : 0) : 1;
+            a.discard_in = in_scratch && keep ? 1 : 0;
         }
         const int ci = a.in_row ? 0 : 1, co = a.out_row ? 0 : 1;
         RecLaunch r;
