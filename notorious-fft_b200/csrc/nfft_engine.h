@@ -285,6 +285,11 @@ const LeanRegistry& lean_registry();
 // Launch the specialized kernel for this pass shape, or return false with no
 // error set when none is instantiated (the caller then uses pass_kernel).
 bool lean_available(int logR, int logT, int ci, int co, int ld, int st);
+// Bluestein middle kernels (nfft_mid.cu): forward last pass + filter product +
+// first pass of the second FFT in one launch (a1 / a2: the two passes).
+bool lean_mid_available(int logR);
+bool mid_set_attributes();
+bool launch_lean_mid(PassArgs a1, PassArgs a2, int logR, cudaStream_t s);
 bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, long long ntiles, cudaStream_t s);
 
 }  // namespace nfft

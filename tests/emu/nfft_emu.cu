@@ -468,6 +468,99 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
     }
 }
 
+template <typename X> struct template_type_tag { using type = X; };
+// ---- Bluestein middle kernels (lean_mid_tile of nfft_lean.cuh): the forward
+// last pass, the filter product and the second FFT's first pass, every phase
+// for all threads; the two passes' line maps must agree.
+static long long g_mid_launches = 0;
+template <int LOGR, int LOGT>
+static void emu_lean_mid(const PassArgs& a1, const PassArgs& a2) {
+    using T = real_t;
+    using V = C2<T>;
+    using Mid = LeanMid<T, LOGR, LOGT>;
+    using L1 = typename Mid::L1;
+    using L2 = typename Mid::L2;
+    const TwTables<T>* tw = (const TwTables<T>*)a1.tw;
+    constexpr int TH = Mid::THREADS;
+    g_smem_elems = L1::SMEM_ELEMS;
+    std::vector<V> sm(L1::SMEM_ELEMS);
+    std::vector<LeanLine> lines(Mid::J);
+    std::vector<V> regs((size_t)TH * 16);
+    std::vector<int> ls((size_t)TH * 16), is((size_t)TH * 16);
+    auto stage = [&](auto Lc, auto Sc, auto Cc, bool to_global, const PassArgs& a) {
+        using L = typename decltype(Lc)::type;
+        constexpr int S = decltype(Sc)::value;
+        constexpr bool COLMAP = decltype(Cc)::value;
+        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
+        for (int t = 0; t < TH; ++t)
+            for (int q = 0; q < 16 / RHO; ++q)
+                L::template read<S, COLMAP>(sm.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
+        for (int t = 0; t < TH; ++t)
+            for (int q = 0; q < 16 / RHO; ++q) {
+                L::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
+                if (to_global)
+                    L::template write_global<S>(a, tw, lines.data(), ls[t * 16 + q], is[t * 16 + q],
+                                                &regs[t * 16 + q * RHO]);
+                else
+                    L::template write_smem<S>(sm.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
+            }
+    };
+    template_type_tag<L1> t1;
+    template_type_tag<L2> t2;
+    const long long ntiles = (a1.nlines + Mid::J - 1) >> Mid::LOGJ;
+    if (a1.nlines != a2.nlines || a1.logJ != Mid::LOGJ || a2.logJ != Mid::LOGJ) {
+        fprintf(stderr, "nfft_emu: Bluestein middle passes disagree on their lines\n");
+        abort();
+    }
+    g_launches++;
+    g_mid_launches++;
+    for (long long tile = 0; tile < ntiles; ++tile) {
+        for (auto& x : sm) x = mkc((T)NAN, (T)NAN);
+        for (int t = 0; t < Mid::J; ++t) {
+            long long u1[3], u2[3];
+            line_setup(a1, (tile << Mid::LOGJ) + t, 0, TileLines{&u1[0], &u1[1], &u1[2]});
+            line_setup(a2, (tile << Mid::LOGJ) + t, 0, TileLines{&u2[0], &u2[1], &u2[2]});
+            if (u1[2] != u2[2]) {
+                fprintf(stderr, "nfft_emu: Bluestein middle line %lld differs between the passes\n", (tile << Mid::LOGJ) + t);
+                abort();
+            }
+            lines[t] = LeanLine{u1[0], u2[1], u1[2]};
+        }
+        for (int t = 0; t < TH; ++t) {
+            L1::first(a1, tw, lines.data(), t, &regs[t * 16], ls[t * 16], is[t * 16]);
+            L1::template write_smem<0>(sm.data(), ls[t * 16], is[t * 16], &regs[t * 16]);
+        }
+        if constexpr (L1::NS >= 3) stage(t1, std::integral_constant<int, 1>{}, std::true_type{}, false, a1);
+        if constexpr (L1::NS >= 4) stage(t1, std::integral_constant<int, 2>{}, std::true_type{}, false, a1);
+        stage(t1, std::integral_constant<int, L1::NS - 1>{}, std::true_type{}, false, a1);
+        for (int e = 0; e < (Mid::J << LOGR); ++e) Mid::filter(a1, sm.data(), lines.data(), e);
+        for (int t = 0; t < TH; ++t) L2::template read<0, true>(sm.data(), t, 0, &regs[t * 16], ls[t * 16], is[t * 16]);
+        for (int t = 0; t < TH; ++t) {
+            L2::pre_twiddle_dft(a2, tw, 0, is[t * 16], &regs[t * 16]);
+            L2::template write_smem<0>(sm.data(), ls[t * 16], is[t * 16], &regs[t * 16]);
+        }
+        if constexpr (L2::NS >= 3) stage(t2, std::integral_constant<int, 1>{}, std::true_type{}, false, a2);
+        if constexpr (L2::NS >= 4) stage(t2, std::integral_constant<int, 2>{}, std::true_type{}, false, a2);
+        stage(t2, std::integral_constant<int, L2::NS - 1>{}, std::false_type{}, true, a2);
+    }
+}
+bool lean_mid_available(int logR) { return logR >= 5 && logR <= 10; }
+bool mid_set_attributes() { return true; }
+bool launch_lean_mid(PassArgs a1, PassArgs a2, int logR, cudaStream_t) {
+    const int logt = logR <= 8 ? 7 : 8;
+    a1.logJ = a2.logJ = logt + 4 - logR;
+    switch (logR) {
+    case 5: emu_lean_mid<5, 7>(a1, a2); return true;
+    case 6: emu_lean_mid<6, 7>(a1, a2); return true;
+    case 7: emu_lean_mid<7, 7>(a1, a2); return true;
+    case 8: emu_lean_mid<8, 7>(a1, a2); return true;
+    case 9: emu_lean_mid<9, 8>(a1, a2); return true;
+    case 10: emu_lean_mid<10, 8>(a1, a2); return true;
+    }
+    set_error(6, "no Bluestein middle kernel for radix 2^%d", logR);
+    return false;
+}
+
 // Middle and last sub-stages of a lean pass (nfft_cluster.cuh lean_tail),
 // every phase for all threads.
 template <typename P, bool TO_GLOBAL>
@@ -1079,4 +1172,5 @@ long long nfft_emu_checks(void) { return emu::n_checks; }
 long long nfft_emu_queue_items(void) { return nfft::g_queue_items; }
 long long nfft_emu_resident_launches(void) { return nfft::g_resident_launches; }
 long long nfft_emu_resident_tma_launches(void) { return nfft::g_resident_tma_launches; }
+long long nfft_emu_mid_launches(void) { return nfft::g_mid_launches; }
 }
