@@ -317,6 +317,56 @@ constexpr size_t lean_smem_bytes() {
     return sizeof(C2<T>) * (size_t)L::SMEM_ELEMS + sizeof(LeanLine) * (size_t)L::J;
 }
 
+// Mirror tile unpack, the items of thread t: (J/2 low lines) x R items, each
+// emitting bins k and M - k; lines fastest, so neighbouring threads write
+// neighbouring bins.  A thread's items share one line and step r by
+// D = THREADS / (J/2), so k steps by D ns and the twiddles follow exactly
+// known ratios: W_N^{k + D ns} = W_N^k W_{2R}^D and e^{-i pi (k + D ns) / 2N} =
+// e^{-i pi k / 2N} W_{8R}^D (N = 2 ns R) -- chains of at most 8 products from
+// one table twiddle.  The self-paired line 0 of tile 0 (bins r ns, then ns/2 +
+// r ns) takes its twiddles from the table.
+template <typename L, typename T, int STORE>
+NFFT_HD void mirror_unpack_thread(const PassArgs& a, const TwTables<T>* tw, const C2<T>* sm, const LeanLine* lines,
+                                  long long tile, int t) {
+    using V = C2<T>;
+    constexpr int LOGR = L::LOGR_;
+    constexpr int R = 1 << LOGR;
+    constexpr int H = L::J / 2;
+    constexpr int ITEMS = H << LOGR;
+    static_assert(L::THREADS % H == 0, "a thread's items share one line");
+    constexpr int D = L::THREADS / H;
+    const long long ns = 1ll << a.logNj, tpt = ns >> L::LOGJ;
+    const long long tt = tile - (tile / tpt) * tpt;
+    const long long M = ns << LOGR;
+    const int l = t & (H - 1);
+    const LeanLine ln = lines[l];
+    auto zget = [&](long long q) {
+        const long long j = q & (ns - 1);
+        const int rr = (int)(q >> a.logNj);
+        return sm[NFFT_SM((lean_idx<true, LOGR, L::LOGJ>(mirror_local(tt, j, L::J, ns), rr)))];
+    };
+    if (tt == 0 && l == 0) {
+        for (int w = t; w < ITEMS; w += L::THREADS)
+            unpack_pair<T, STORE>(a, tw, ln.bout, mirror_item_k(tt, l, w >> (L::LOGJ - 1), R, ns, ln.j), M, zget);
+        return;
+    }
+    const V ws = twiddle<T>(tw, (uint64_t)D, LOGR + 1);   // W_{2R}^D
+    V ts = V{};
+    if constexpr (STORE == ST_T2) ts = twiddle<T>(tw, (uint64_t)D, LOGR + 3);   // W_{8R}^D
+    V wk = V{}, tk = V{};
+    for (int w = t; w < ITEMS; w += L::THREADS) {
+        const long long k = mirror_item_k(tt, l, w >> (L::LOGJ - 1), R, ns, ln.j);
+        if (w == t) {
+            wk = twiddle<T>(tw, (uint64_t)k, a.logN);
+            if constexpr (STORE == ST_T2) tk = twiddle<T>(tw, (uint64_t)k, a.logN + 2);
+        } else {
+            wk = cmul(wk, ws);
+            if constexpr (STORE == ST_T2) tk = cmul(tk, ts);
+        }
+        unpack_pair_tw<T, STORE>(a, tw, ln.bout, k, M, zget, wk, tk);
+    }
+}
+
 // One tile of a specialized pass (all threads of the CTA call it; uniform
 // early exit past the last line).
 template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
@@ -419,22 +469,7 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
     }
     if constexpr (L::MIRROR) {
         __syncthreads();
-        // mirror tile: (J/2 low lines) x R unpack items, each emitting bins k, M - k;
-        // lines fastest, so neighbouring threads write neighbouring bins
-        const long long ns = 1ll << a.logNj, tpt = ns >> L::LOGJ;
-        const long long tt = tile - (tile / tpt) * tpt;
-        const long long M = ns << LOGR;
-        constexpr int ITEMS = (L::J / 2) << LOGR;
-        for (int w = t; w < ITEMS; w += L::THREADS) {
-            const int l = w & (L::J / 2 - 1), r = w >> (L::LOGJ - 1);
-            const LeanLine ln = lines[l];
-            const long long k = mirror_item_k(tt, l, r, 1 << LOGR, ns, ln.j);
-            unpack_pair<T, STORE>(a, tw, ln.bout, k, M, [&](long long q) {
-                const long long j = q & (ns - 1);
-                const int rr = (int)(q >> a.logNj);
-                return sm[NFFT_SM((lean_idx<true, LOGR, L::LOGJ>(mirror_local(tt, j, L::J, ns), rr)))];
-            });
-        }
+        mirror_unpack_thread<L, T, STORE>(a, tw, sm, lines, tile, t);
     } else if constexpr (L::PAIRED) {
         __syncthreads();
         // whole lines in row layout: realdft unpack / DCT-2 post pairs

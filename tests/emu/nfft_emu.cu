@@ -439,22 +439,7 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
                 }
         }
         if constexpr (Lt::MIRROR) {
-            const long long M = ns << LOGR;
-            constexpr int ITEMS = (Lt::J / 2) << LOGR;
-            for (int w = 0; w < ITEMS; ++w) {
-                const int l = w & (Lt::J / 2 - 1), r = w >> (Lt::LOGJ - 1);
-                const LeanLine ln = lines[l];
-                const long long k = mirror_item_k(tt, l, r, 1 << LOGR, ns, ln.j);
-                unpack_pair<T, ST>(a, tw, ln.bout, k, M, [&](long long q) {
-                    const long long j = q & (ns - 1);
-                    const int ll = mirror_local(tt, j, Lt::J, ns);
-                    if (ll < 0 || ll >= Lt::J || lines[ll].j != j) {
-                        fprintf(stderr, "nfft_emu: mirror unpack reads line %lld outside its tile\n", j);
-                        abort();
-                    }
-                    return sm[NFFT_SM((lean_idx<true, LOGR, Lt::LOGJ>(ll, (int)(q >> a.logNj))))];
-                });
-            }
+            for (int t = 0; t < TH; ++t) mirror_unpack_thread<Lt, T, ST>(a, tw, sm.data(), lines.data(), tile, t);
         } else if constexpr (Lt::PAIRED) {
             constexpr int ITEMS = Lt::J << (LOGR - 1);
             for (int w = 0; w < ITEMS; ++w) {
