@@ -367,6 +367,48 @@ NFFT_HD void mirror_unpack_thread(const PassArgs& a, const TwTables<T>* tw, cons
     }
 }
 
+// Row-tile paired unpack (whole lines: realdft unpack / DCT-2 post pairs), the
+// items of thread t: item w is the bin pair k, R - k (k = w mod (R/2)) of line
+// w / (R/2), R the packed spectrum length.  With
+// R/2 > THREADS a thread walks one line at a time with k stepping by THREADS
+// (twiddles times the exact ratios W_N^THREADS and e^{-i pi THREADS / 2N}, at
+// most 8 products per line); otherwise its k is the same on every line and the
+// twiddles are reused.  Bin 0 (with bins M and M/2) goes through unpack_pair.
+template <typename L, typename T, int STORE>
+NFFT_HD void paired_unpack_thread(const PassArgs& a, const TwTables<T>* tw, const C2<T>* sm, const LeanLine* lines,
+                                  int t) {
+    using V = C2<T>;
+    constexpr int LOGR = L::LOGR_;
+    constexpr int HALF = LOGR == 0 ? 1 : (1 << (LOGR - 1));
+    constexpr int ITEMS = L::J * HALF;
+    V ws = V{}, ts = V{};
+    if constexpr (HALF > L::THREADS) {
+        ws = twiddle<T>(tw, (uint64_t)L::THREADS, a.logN);
+        if constexpr (STORE == ST_T2) ts = twiddle<T>(tw, (uint64_t)L::THREADS, a.logN + 2);
+    }
+    V wk = V{}, tk = V{};
+    int prevk = -1;
+    for (int w = t; w < ITEMS; w += L::THREADS) {
+        const int ll = w / HALF, k = w & (HALF - 1);
+        const LeanLine ln = lines[ll];
+        if (ln.j < 0) continue;
+        auto zget = [&](long long r) { return sm[NFFT_SM((lean_idx<false, LOGR, L::LOGJ>(ll, (int)r)))]; };
+        if (k == 0) {
+            unpack_pair<T, STORE>(a, tw, ln.bout, 0, (long long)(1 << LOGR), zget);
+            continue;
+        }
+        if (prevk < 0 || k < prevk) {
+            wk = twiddle<T>(tw, (uint64_t)k, a.logN);
+            if constexpr (STORE == ST_T2) tk = twiddle<T>(tw, (uint64_t)k, a.logN + 2);
+        } else if (k != prevk) {
+            wk = cmul(wk, ws);
+            if constexpr (STORE == ST_T2) tk = cmul(tk, ts);
+        }
+        prevk = k;
+        unpack_pair_tw<T, STORE>(a, tw, ln.bout, k, (long long)(1 << LOGR), zget, wk, tk);
+    }
+}
+
 // One tile of a specialized pass (all threads of the CTA call it; uniform
 // early exit past the last line).
 template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
@@ -472,15 +514,7 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
         mirror_unpack_thread<L, T, STORE>(a, tw, sm, lines, tile, t);
     } else if constexpr (L::PAIRED) {
         __syncthreads();
-        // whole lines in row layout: realdft unpack / DCT-2 post pairs
-        constexpr int ITEMS = (LOGR == 0) ? L::J : (L::J << (LOGR - 1));
-        for (int w = t; w < ITEMS; w += L::THREADS) {
-            int ll = w >> (LOGR - 1), k = w & ((1 << (LOGR - 1)) - 1);
-            const LeanLine ln = lines[ll];
-            if (ln.j < 0) continue;
-            unpack_pair<T, STORE>(a, tw, ln.bout, k, (long long)(1 << LOGR),
-                                  [&](long long r) { return sm[NFFT_SM((lean_idx<false, LOGR, L::LOGJ>(ll, (int)r)))]; });
-        }
+        paired_unpack_thread<L, T, STORE>(a, tw, sm, lines, t);
     }
 }
 

@@ -441,14 +441,7 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
         if constexpr (Lt::MIRROR) {
             for (int t = 0; t < TH; ++t) mirror_unpack_thread<Lt, T, ST>(a, tw, sm.data(), lines.data(), tile, t);
         } else if constexpr (Lt::PAIRED) {
-            constexpr int ITEMS = Lt::J << (LOGR - 1);
-            for (int w = 0; w < ITEMS; ++w) {
-                int ll = w >> (LOGR - 1), k = w & ((1 << (LOGR - 1)) - 1);
-                const LeanLine ln = lines[ll];
-                if (ln.j < 0) continue;
-                unpack_pair<T, ST>(a, tw, ln.bout, k, (long long)(1 << LOGR),
-                                   [&](long long r) { return sm[NFFT_SM((lean_idx<false, LOGR, Lt::LOGJ>(ll, (int)r)))]; });
-            }
+            for (int t = 0; t < TH; ++t) paired_unpack_thread<Lt, T, ST>(a, tw, sm.data(), lines.data(), t);
         }
     }
 }
