@@ -158,6 +158,40 @@ struct Lean {
 #pragma unroll
                 for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
             }
+        } else if constexpr ((LOAD == LD_R2C || LOAD == LD_T2) && !COL_IN) {
+            // row tile of a single-pass real transform (line j = 0): the packed
+            // point p = i + m R/16 of the line's N = 2R reals, without the generic
+            // operator's per-element branches
+            const T* x = (const T*)a.in + ln.bin;
+            if (a.in_estride == 1 && ln.j == 0) {
+                if constexpr (LOAD == LD_R2C) {
+                    if (((uintptr_t)x & (sizeof(C2<T>) - 1)) == 0) {
+#pragma unroll
+                        for (int m = 0; m < 16; ++m) v[m] = NFFT_GLD((const C2<T>*)x + i + (m << (LOGR - 4)));
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < 16; ++m) {
+                            const long long q = 2 * (long long)(i + (m << (LOGR - 4)));
+                            v[m] = mkc(NFFT_GLD(&x[q]), NFFT_GLD(&x[q + 1]));
+                        }
+                    }
+                } else {
+                    // DCT-2 / DST-2 reorder v[i] = x[2i] (i < N/2), +-x[2N-1-2i]: points
+                    // m < 8 lie in the first half of the packed line, m >= 8 in the second
+                    const long long N2 = 2 * a.N;
+                    const T sg = a.dst ? (T)-1 : (T)1;
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        const long long q = 4 * (long long)(i + (m << (LOGR - 4)));
+                        if (m < 8) v[m] = mkc(NFFT_GLD(&x[q]), NFFT_GLD(&x[q + 2]));
+                        else v[m] = mkc(sg * NFFT_GLD(&x[N2 - 1 - q]), sg * NFFT_GLD(&x[N2 - 3 - q]));
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < 16; ++m)
+                    v[m] = load_elem<T, LOAD>(a, tw, ln.bin, ln.j + ((long long)(i + (m << (LOGR - 4))) << a.logNj));
+            }
         } else {
 #pragma unroll
             for (int m = 0; m < 16; ++m)
