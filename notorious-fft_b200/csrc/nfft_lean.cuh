@@ -158,6 +158,28 @@ struct Lean {
 #pragma unroll
                 for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
             }
+        } else if constexpr (LOAD == LD_T4 && !COL_IN) {
+            // row tile of a single-pass DCT-4 / DST-4 (line j = 0): premultiply
+            // e^{-i pi p / N} of p = i + m R/16 as a chain of exact steps
+            // e^{-i pi (R/16) / N} = W_64 (N = 2R) from one table twiddle
+            const T* x = (const T*)a.in + ln.bin;
+            if (a.in_estride == 1 && ln.j == 0) {
+                const long long N = a.N;
+                C2<T> e = twiddle<T>(tw, (uint64_t)i, a.logN + 1);
+                const C2<T> st = twiddle<T>(tw, (uint64_t)1, 6);
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const long long p = i + (m << (LOGR - 4));
+                    const T xe = NFFT_GLD(&x[2 * p]), xo = NFFT_GLD(&x[N - 1 - 2 * p]);
+                    if (!a.dst) v[m] = mkc(e.x * xe - e.y * xo, e.x * xo + e.y * xe);
+                    else v[m] = mkc(-e.x * xe - e.y * xo, e.x * xo - e.y * xe);
+                    if (m < 15) e = cmul(e, st);
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < 16; ++m)
+                    v[m] = load_elem<T, LOAD>(a, tw, ln.bin, ln.j + ((long long)(i + (m << (LOGR - 4))) << a.logNj));
+            }
         } else if constexpr ((LOAD == LD_R2C || LOAD == LD_T2) && !COL_IN) {
             // row tile of a single-pass real transform (line j = 0): the packed
             // point p = i + m R/16 of the line's N = 2R reals, without the generic

@@ -243,7 +243,8 @@ NFFT_HD void store_elem(const PassArgs& a, const TwTables<T>* tw, long long base
         T* y = (T*)a.out + base;
         const long long es = a.out_estride, N = a.N;
         V f0 = twiddle<T>(tw, (uint64_t)(4 * q + 1), a.logN + 3);
-        V f1 = twiddle<T>(tw, (uint64_t)(2 * N - 1 - 4 * q), a.logN + 3);
+        // f(N-1-2q) = e^{-i pi / 2} conj f(2q) exactly
+        V f1 = mkc(-f0.y, -f0.x);
         V c = cconj(v);
         T y0, y1;
         if (!a.dst) {
