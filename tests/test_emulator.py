@@ -274,3 +274,29 @@ def test_emu_bluestein_fused_middle(emu_d, emu_f, oracle_d, single, n, batch, mo
             for b in range(batch):
                 assert rel_l2(y[b], oracle_d.transform(k, x[b].astype(np.complex128))) <= lim, (k, b)
     assert f() - m0 == 2
+
+
+@pytest.mark.parametrize("single", [False, True])
+@pytest.mark.parametrize("n", [64, 1024, 8192])
+def test_emu_real_rows_odd_batch_stride(emu_d, emu_f, oracle_d, n, single):
+    """Batched single-pass real transforms whose input stride is odd: every other
+    transform starts off the vector boundary (the packed realdft row loads fall
+    back to scalar loads there); realdft, DCT-2 / DST-2, DCT-4 / DST-4."""
+    lib = emu_f if single else emu_d
+    B, idist = 3, n + 1
+    rng = np.random.default_rng(n + 7)
+    x = rng.uniform(-1, 1, B * idist).astype(lib.rdt)
+    with lib.mkaux("realdft", [n]) as a:
+        z = np.zeros(B * (n // 2 + 1), lib.cdt)
+        a.batched("realdft", x, z, B, idist, n // 2 + 1)
+        for b in range(B):
+            ref = oracle_d.transform("realdft", x[b * idist: b * idist + n].astype(np.float64))
+            assert rel_l2(z[b * (n // 2 + 1):(b + 1) * (n // 2 + 1)], ref) <= tol(n, single), b
+    for fam, kinds in (("t2t3", ("dct2", "dst2")), ("t4", ("dct4", "dst4"))):
+        with lib.mkaux(fam, [n]) as a:
+            for k in kinds:
+                y = np.zeros(B * n, lib.rdt)
+                a.batched(k, x, y, B, idist, n)
+                for b in range(B):
+                    ref = oracle_d.transform(k, x[b * idist: b * idist + n].astype(np.float64))
+                    assert rel_l2(y[b * n:(b + 1) * n], ref) <= tol(n, single), (k, b)

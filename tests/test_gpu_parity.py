@@ -320,3 +320,29 @@ def test_bluestein_fused_middle(lib_d, lib_f, oracle_d, single, n, batch, monkey
             a.batched(k, x, y, batch, n, n)
             for b in (0, batch - 1):
                 assert rel_l2(y[b], oracle_d.transform(k, x[b].astype(np.complex128))) <= lim, (k, b)
+
+
+@pytest.mark.parametrize("single", [False, True])
+@pytest.mark.parametrize("n", [64, 4096, 16384])
+def test_real_rows_odd_batch_stride(lib_d, lib_f, oracle_d, single, n):
+    """Batched single-pass real transforms with an odd input stride (every other
+    transform off the 16-byte boundary): realdft, DCT-2 / DST-2, DCT-4 / DST-4."""
+    lib = lib_f if single else lib_d
+    lim = (1e-6 if single else 1e-13) * max(1.0, math.log2(n))
+    B, idist = 5, n + 1
+    rng = np.random.default_rng(n + 9)
+    x = rng.uniform(-1, 1, B * idist).astype(lib.rdt)
+    with lib.mkaux("realdft", [n]) as a:
+        z = np.zeros(B * (n // 2 + 1), lib.cdt)
+        a.batched("realdft", x, z, B, idist, n // 2 + 1)
+        for b in range(B):
+            ref = oracle_d.transform("realdft", x[b * idist: b * idist + n].astype(np.float64))
+            assert rel_l2(z[b * (n // 2 + 1):(b + 1) * (n // 2 + 1)], ref) <= lim, b
+    for fam, kinds in (("t2t3", ("dct2", "dst2")), ("t4", ("dct4", "dst4"))):
+        with lib.mkaux(fam, [n]) as a:
+            for k in kinds:
+                y = np.zeros(B * n, lib.rdt)
+                a.batched(k, x, y, B, idist, n)
+                for b in range(B):
+                    ref = oracle_d.transform(k, x[b * idist: b * idist + n].astype(np.float64))
+                    assert rel_l2(y[b * n:(b + 1) * n], ref) <= lim, (k, b)
