@@ -10,6 +10,7 @@ differences.  Tolerances are the north-star ones (1e-13 log2 N for double,
 1e-6 log2 N for float).
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -300,3 +301,31 @@ def test_emu_real_rows_odd_batch_stride(emu_d, emu_f, oracle_d, n, single):
                 for b in range(B):
                     ref = oracle_d.transform(k, x[b * idist: b * idist + n].astype(np.float64))
                     assert rel_l2(y[b * n:(b + 1) * n], ref) <= tol(n, single), (k, b)
+
+
+def test_emu_pass_cap_override_keeps_four_passes(tmp_path):
+    """NOTORIOUS_FFT_MAX_PASS_LOG=4 on a 2^17 axis would ask for five passes;
+    the schedule holds four, so the cap is raised to ceil(17 / 4) and the
+    transform stays exact (child process: the switch is read once)."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    child = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from notorious_fft import Library
+L = Library(sys.argv[2])
+n = 1 << 17
+rng = np.random.default_rng(3)
+x = rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
+with L.mkaux("dft", [n]) as a:
+    y = a("dft", x)
+ref = np.fft.fft(x)
+print(float(np.linalg.norm(y - ref) / np.linalg.norm(ref)))
+"""
+    env = dict(os.environ, NOTORIOUS_FFT_MAX_PASS_LOG="4")
+    r = subprocess.run([sys.executable, "-c", child, os.path.join(root, "notorious-fft_b200"),
+                        os.path.join(root, "tests", "emu", "_build", "libnfft_emu_d.so")],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert float(r.stdout.strip().splitlines()[-1]) < 1e-13 * 17
