@@ -108,6 +108,36 @@ bool run_pipelined(notorious_fft_plan* p, int kind, const void* x, void* y, long
     return ok;
 }
 
+// Calls on one plan share its device scratch.  Calls on one stream are
+// ordered by that stream; a call on a different stream than the previous
+// call first waits for the previous call's work (an event recorded at the end
+// of every call).  Streams being captured into a CUDA graph are neither made
+// to wait nor recorded: ordering a capture against earlier calls on other
+// streams is the caller's (synchronize before capturing).
+bool is_capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return st != cudaStreamCaptureStatusNone;
+}
+
+bool order_after_previous_call(notorious_fft_plan* p, cudaStream_t s, bool capturing) {
+    if (capturing || !p->ev_pending || p->last_stream == s) return true;
+    return cuda_ok(cudaStreamWaitEvent(s, p->ev_last, 0), "cudaStreamWaitEvent(previous call)");
+}
+
+void note_call(notorious_fft_plan* p, cudaStream_t s, bool capturing) {
+    if (capturing) return;
+    if (!p->ev_last && !cuda_ok(cudaEventCreateWithFlags(&p->ev_last, cudaEventDisableTiming), "cudaEventCreate"))
+        return;
+    if (cuda_ok(cudaEventRecord(p->ev_last, s), "cudaEventRecord(call end)")) {
+        p->last_stream = s;
+        p->ev_pending = true;
+    }
+}
+
 bool is_device_ptr(const void* ptr) {
     cudaPointerAttributes attr;
     cudaError_t e = cudaPointerGetAttributes(&attr, ptr);
@@ -172,7 +202,16 @@ void run(int kind, const void* x, void* y, const notorious_fft_aux* a, long long
     cudaStream_t s = t_stream;
     const void* din = x;
     void* dout = y;
-    if (!xd && !yd && howmany >= 4 && (x != y || idist == odist) && is_pinned_host_ptr(x) && is_pinned_host_ptr(y)) {
+    const bool capturing = is_capturing(s);
+    // In place (x == y), chunk k's copy-out may land while chunk k+1 is copied
+    // in, so the pipeline is only taken when every transform's output stays
+    // inside its own input slot: equal byte distances and an output no longer
+    // than that distance.  Other in-place layouts take the staged path below.
+    const bool inplace_ok = x != y || ((size_t)idist * in_eb == (size_t)odist * out_eb &&
+                                       (size_t)out_elems * out_eb <= (size_t)idist * in_eb &&
+                                       (size_t)in_elems * in_eb <= (size_t)idist * in_eb);
+    if (!order_after_previous_call(p, s, capturing)) goto done;
+    if (!xd && !yd && howmany >= 4 && inplace_ok && is_pinned_host_ptr(x) && is_pinned_host_ptr(y)) {
         run_pipelined(p, kind, x, y, howmany, idist, odist, in_elems, out_elems, in_eb, out_eb, vjp, s);
         goto done;
     }
@@ -207,6 +246,7 @@ void run(int kind, const void* x, void* y, const notorious_fft_aux* a, long long
     }
     if (!xd || !yd) cuda_ok(cudaStreamSynchronize(s), "stream synchronize");
 done:
+    note_call(p, s, capturing);
     if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
 }
 

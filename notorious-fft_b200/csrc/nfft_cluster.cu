@@ -70,7 +70,7 @@ int prepare(ClusterEntry& e) {
 }  // namespace
 
 bool cluster_available(int logN) {
-    // opt-in: on B200 the two-pass kernels are faster for now
+    // opt-in: on B200 the two-pass kernels measured faster (2^14: 3091 vs 2198 GB/s FP64)
     const char* v = getenv("NOTORIOUS_FFT_CLUSTER");
     if (!v || !atoi(v)) return false;
     ClusterEntry* e = find_cluster(logN);

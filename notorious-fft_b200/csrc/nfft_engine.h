@@ -132,6 +132,12 @@ struct notorious_fft_plan {
     // counters of the resident two-pass kernel
     unsigned* res_ctr = nullptr;
     size_t res_ctr_n = 0;
+    // ordering across streams: the scratch above is shared by every call on
+    // this plan, so a call on another stream than the previous call's first
+    // waits for the event recorded at the end of that call
+    cudaStream_t last_stream = nullptr;
+    cudaEvent_t ev_last = nullptr;
+    bool ev_pending = false;
     std::mutex mu;
 };
 

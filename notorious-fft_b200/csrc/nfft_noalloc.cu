@@ -42,12 +42,16 @@ struct NoallocDevice {
     bool ready = false;
     cplx_t* scratch = nullptr;
     TwTables<real_t>* tw = nullptr;
+    int sm_count = 0;       // read once per device; the pass launcher sizes grids
+    size_t l2_bytes = 0;    // and picks its L2 policy from these, as for plans
 };
 std::mutex g_noalloc_mu;
 NoallocDevice g_noalloc_dev[64];
 
 // One-time set-up of the calling thread's current device (see the file header).
-NoallocDevice* noalloc_device() {
+// The set-up waits for a kernel, so it cannot run while `stream` is being
+// captured into a CUDA graph: such a first call is refused with a message.
+NoallocDevice* noalloc_device(cudaStream_t stream) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
@@ -57,6 +61,23 @@ NoallocDevice* noalloc_device() {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     NoallocDevice& d = g_noalloc_dev[dev];
     if (d.ready) return &d;
+    int major = 0, sms = 0, l2 = 0;
+    if (!cuda_ok(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev), "cudaDeviceGetAttribute") ||
+        !cuda_ok(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute") ||
+        !cuda_ok(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev), "cudaDeviceGetAttribute"))
+        return nullptr;
+    if (major < 10) {
+        set_error(NOTORIOUS_FFT_ERR_NO_DEVICE, "device %d (sm_%d) is not an sm_100 GPU", dev, major);
+        return nullptr;
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (!cuda_ok(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing")) return nullptr;
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error(NOTORIOUS_FFT_ERR_UNSUPPORTED,
+                  "notorious_fft_dft_noalloc: the first call on a device sets up its tables and waits for them; "
+                  "make one call on this device before capturing a stream");
+        return nullptr;
+    }
     void* scratch = nullptr;
     void* tw = nullptr;
     if (!cuda_ok(cudaGetSymbolAddress(&scratch, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)")) return nullptr;
@@ -66,6 +87,8 @@ NoallocDevice* noalloc_device() {
     if (!cuda_ok(cudaStreamSynchronize(0), "twiddle table set-up")) return nullptr;
     d.scratch = (cplx_t*)scratch;
     d.tw = (TwTables<real_t>*)tw;
+    d.sm_count = sms;
+    d.l2_bytes = (size_t)l2;
     d.ready = true;
     return &d;
 }
@@ -95,24 +118,24 @@ extern "C" int notorious_fft_dft_noalloc(const notorious_fft_cmpl* x, notorious_
         return NOTORIOUS_FFT_ERR_INVALID;
     }
     if (howmany == 0) return 0;
-    NoallocDevice* d = noalloc_device();
+    cudaStream_t s = (cudaStream_t)stream;
+    NoallocDevice* d = noalloc_device(s);
     if (!d) return last_error();
     DeviceCtx ctx;
     ctx.tw = d->tw;
-    cudaStream_t s = (cudaStream_t)stream;
+    ctx.sm_count = d->sm_count;
+    ctx.l2_bytes = d->l2_bytes;
     int logN = 0;
     while ((1 << logN) < N) ++logN;
     const long long L = N;
     const long long half = NOALLOC_SCRATCH_ELEMS / 2;
     // The default schedule, unless it runs more than two passes (the passes
     // then alternate between the two halves of the scratch array) and a
-    // transform does not fit in half: then the uncapped two-pass schedule.
+    // transform does not fit in half: then the uncapped two-pass schedule,
+    // which for N <= 2^20 always has at most two passes and so needs only one
+    // buffer of at most the whole array (FP64 2^20 fills it exactly).
     FftSchedule sch = make_schedule(logN, false);
     if (sch.npass > 2 && L > half) sch = make_schedule(logN, false, 13, 0);
-    if (sch.npass > 2 && L > half) {
-        set_error(NOTORIOUS_FFT_ERR_UNSUPPORTED, "schedule needs more than one scratch buffer");
-        return NOTORIOUS_FFT_ERR_UNSUPPORTED;
-    }
     OpSpec op;
     op.conj_in = op.conj_out = inverse ? 1 : 0;
     // whole transforms per scratch fill

@@ -891,6 +891,7 @@ void plan_destroy(notorious_fft_plan* p) {
         if (p->ev_c[i]) cudaEventDestroy(p->ev_c[i]);
         if (p->ev_d[i]) cudaEventDestroy(p->ev_d[i]);
     }
+    if (p->ev_last) cudaEventDestroy(p->ev_last);
     if (p->s_h2d) cudaStreamDestroy(p->s_h2d);
     if (p->s_d2h) cudaStreamDestroy(p->s_d2h);
     if (p->nd_tmp) cudaFree(p->nd_tmp);

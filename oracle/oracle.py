@@ -31,9 +31,25 @@ R2R_KINDS = {"dct2": 2, "dst2": 3, "dct3": 4, "dst3": 5, "dct4": 6, "dst4": 7}
 KINDS = ("dft", "invdft", "realdft", "invrealdft") + tuple(R2R_KINDS)
 
 
+# Where the reference project's sources are read from (its include/ and
+# tests/ directories).  Only the recipes that compile them (oracle/Makefile,
+# tests/refsuite/Makefile) and the compile check of its C++ wrapper read
+# there; every other test uses what they built.  Set NOTORIOUS_FFT_REF_DIR to
+# point elsewhere; without it the conventional read-only mount is used when
+# present.
+_DEFAULT_REF_DIR = "/root/reference"
+
+
+def reference_dir():
+    """The reference sources' directory, or None when they are not present."""
+    d = os.environ.get("NOTORIOUS_FFT_REF_DIR") or _DEFAULT_REF_DIR
+    return d if os.path.exists(os.path.join(d, "include", "notorious_fft.h")) else None
+
+
 def build():
     """Build the C restatement (and the reference, when its sources exist)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    ref = reference_dir()
+    subprocess.run(["make", "-s", "-C", HERE] + ([f"REF={ref}"] if ref else []), check=True)
 
 
 def _ptr(a):

@@ -77,10 +77,13 @@ def test_no_gpu_mkaux_returns_null():
     assert lib.notorious_fft_last_error() != 0
 
 
-REF_HPP = "/root/reference/include/notorious_fft.hpp"
+from oracle import reference_dir  # noqa: E402
+
+_REF = reference_dir()
+REF_HPP = os.path.join(_REF, "include", "notorious_fft.hpp") if _REF else ""
 
 
-@pytest.mark.skipif(not os.path.exists(REF_HPP), reason="reference sources not present")
+@pytest.mark.skipif(not _REF, reason="reference sources not present (set NOTORIOUS_FFT_REF_DIR)")
 @pytest.mark.parametrize("single", [False, True], ids=["double", "float"])
 def test_reference_cpp_wrapper_compiles_against_this_header(tmp_path, single):
     """The reference's C++17 wrapper (include/notorious_fft.hpp) builds
