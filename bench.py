@@ -107,57 +107,87 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_reference(kind_pairs, N, sample, threads, reps=3, lib="libref_d_avx2.so", prec="f64"):
-    """Time the reference's own CPU path (oracle/_ref, compiled from the
-    reference sources) on the host cores.  Returns (seconds per transform
-    summed over kind_pairs, kind)."""
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def cpu_run(kinds, dims, batch, threads, reps, lib="libref_d_avx2.so", prec="f64", listfile=None):
+    """Run the reference's own CPU path (oracle/_ref, compiled from the
+    reference sources) through oracle/_build/cpu_bench on the host cores.
+    Returns the harness's JSON record (best-of-reps seconds and every rep's
+    seconds), or None when the reference build is missing."""
     exe = os.path.join(ROOT, "oracle", "_build", "cpu_bench")
     so = os.path.join(ROOT, "oracle", "_ref", lib)
-    kind = "reference"
     if not (os.path.exists(exe) and os.path.exists(so)):
-        return None, "unavailable"
-    total = 0.0
-    for k in kind_pairs:
-        r = subprocess.run([exe, so, prec, k, str(N), str(sample), str(threads), str(reps)], capture_output=True,
-                           text=True, timeout=600)
-        if r.returncode != 0:
-            return None, "unavailable"
-        d = json.loads(r.stdout.strip().splitlines()[-1])
-        total += d["seconds"] / sample
-    return total, kind
+        return None
+    if listfile is not None:
+        cmd = [exe, so, prec, "ragged", listfile, "-", str(threads), str(reps)]
+    else:
+        cmd = [exe, so, prec, ",".join(kinds), "x".join(map(str, dims)), str(batch), str(threads), str(reps)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return None
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def cpu_entry(rec, nbytes, sample, lib, threads, extra=None):
+    """A configuration's cpu_baseline object from a cpu_bench record."""
+    if rec is None:
+        return {"unavailable": "reference CPU build missing (oracle/_ref)"}
+    e = {"ms": round(rec["seconds"] * 1e3, 3), "gb_s": round(nbytes / rec["seconds"] / 1e9, 2),
+         "cores": threads, "cpu": cpu_model(), "kind": "reference", "build": lib, "sample": sample}
+    if extra:
+        e.update(extra)
+    return e
 
 
 def run_reference_arm(args, wl):
+    """The reference's own CPU implementation of the workload, timed on the
+    host cores: every step is the whole batch (dft then invdft of all its
+    transforms), OpenMP over the batch with one aux per thread, the
+    reference built -O3 -fopenmp -mavx2 -mfma from its sources.  The first W
+    reps are warm-up; the K reps after them are the timed steps."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    N = wl["N"]
-    sample = max(threads * 4, 64) if N >= 65536 else 1024
-    per = []
-    for _ in range(args.warmup):
-        cpu_reference(["dft", "invdft"], N, sample, threads, reps=1)
+    threads = host_cores()
+    N, B = wl["N"], wl["batch"]
     t0 = time.time()
-    for _ in range(args.steps):
-        s, kind = cpu_reference(["dft", "invdft"], N, sample, threads, reps=1)
-        if s is None:
-            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build missing (oracle/_ref)"}))
-            return
-        per.append(s)
-    sec = statistics.median(per)          # seconds for one dft + one invdft
-    bytes_per_pair = 2 * 2 * N * 16
-    gbs = bytes_per_pair / sec / 1e9
-    ms_step = sec * wl["batch"] * 1e3
+    rec = cpu_run(["dft", "invdft"], [N], B, threads, args.warmup + args.steps)
+    if rec is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build missing (oracle/_ref)"}))
+        return
+    steps = rec["rep_seconds"][args.warmup:]
+    sec = sum(steps) / len(steps)
+    bytes_per_step = 2 * B * 2 * N * 16
+    gbs = bytes_per_step / sec / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"c2c fp64 N={N} x{wl['batch']} dft+invdft (reference CPU path)", "N": N,
-                   "batch": wl["batch"], "l2": wl["l2"]},
-        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-                         "sample": f"{sample} transforms per direction per step, OpenMP over the batch, "
-                                   f"one aux per thread, -O3 -fopenmp -mavx2 -mfma"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (uniform[-1,1), splitmix64 seeded)",
+        "config": {"workload": f"c2c fp64 N={N} x{B} dft+invdft per GPU", "N": N, "batch": B, "l2": wl["l2"],
+                   "parallelism": f"batch-sharded x{world}"},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "cpu": cpu_model(),
+                         "kind": "reference",
+                         "sample": f"the whole batch every step ({B} x dft then {B} x invdft in place, N={N}), "
+                                   f"OpenMP over the batch with one aux per thread, "
+                                   f"reference built -O3 -fopenmp -mavx2 -mfma"},
         "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_seconds": [round(t, 4) for t in steps],
         "wall_s": round(time.time() - t0, 2),
     }
     print(json.dumps(line))
@@ -314,6 +344,16 @@ def bench_configs(args, stream):
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
     out = {}
+    T = host_cores()
+    cpu_on = not args.no_cpu
+
+    def cpu(kinds, dims, batch, nbytes, sample, threads=None, lib="libref_d_avx2.so", prec="f64", reps=3, **kw):
+        """The reference's CPU path on the same configuration (same run, host cores)."""
+        if not cpu_on:
+            return None
+        th = T if threads is None else threads
+        rec = cpu_run(kinds, dims, batch, th, reps, lib=lib, prec=prec, **kw)
+        return cpu_entry(rec, nbytes, sample, lib, th)
 
     def entry(name, ms, nbytes, err, **kw):
         e = {"ms": round(ms, 4), "gb_s": round(nbytes / (ms * 1e-3) / 1e9, 1), "max_rel_l2": err}
@@ -327,7 +367,9 @@ def bench_configs(args, stream):
         ms = timed(lambda: (a.batched("dft", x, y, 256, 4096, 4096), a.batched("invdft", y, z, 256, 4096, 4096)))
         torch.cuda.synchronize()
         err = rel(y[:4].cpu(), torch.fft.fft(x[:4], dim=1).cpu())
-    entry("c1_dft_invdft_4096x256_f64", ms, 2 * 256 * 4096 * 32, err)
+    entry("c1_dft_invdft_4096x256_f64", ms, 2 * 256 * 4096 * 32, err,
+          cpu_baseline=cpu(["dft", "invdft"], [4096], 256, 2 * 256 * 4096 * 32,
+                           "256 x dft then invdft in place, OpenMP over the batch, one aux per thread"))
     del x, y, z
 
     # C2: realdft 2^20 x 16
@@ -338,7 +380,9 @@ def bench_configs(args, stream):
         ms = timed(lambda: a.batched("realdft", x, zc, 16, n, n // 2 + 1))
         torch.cuda.synchronize()
         err = rel(zc[:2].cpu(), torch.fft.rfft(x[:2], dim=1).cpu())
-    entry("c2_realdft_1048576x16_f64", ms, 16 * (n * 8 + (n // 2 + 1) * 16), err)
+    entry("c2_realdft_1048576x16_f64", ms, 16 * (n * 8 + (n // 2 + 1) * 16), err,
+          cpu_baseline=cpu(["realdft"], [n], 16, 16 * (n * 8 + (n // 2 + 1) * 16),
+                           "16 transforms, OpenMP over the batch, one aux per thread"))
     del x, zc
     # C2: DCT-2 / DST-2 / DCT-4, 8192 x 512
     n, b = 8192, 512
@@ -351,7 +395,8 @@ def bench_configs(args, stream):
             torch.cuda.synchronize()
             xs, ys = x[:2].cpu().numpy(), y[:2].cpu().numpy()
             err = max(rel(ys[i], ref(xs[i])) for i in range(2))
-        entry(f"c2_{kind}_8192x512_f64", ms, b * n * 16, err)
+        entry(f"c2_{kind}_8192x512_f64", ms, b * n * 16, err,
+              cpu_baseline=cpu([kind], [n], b, b * n * 16, "512 transforms, OpenMP over the batch, one aux per thread"))
     del x, y
     # C2: 2-D 2048^2 and 3-D 256^3 complex
     for dims in ((2048, 2048), (256, 256, 256)):
@@ -361,7 +406,10 @@ def bench_configs(args, stream):
             ms = timed(lambda: a("dft", x, y))
             torch.cuda.synchronize()
             err = rel(y.cpu(), torch.fft.fftn(x).cpu())
-        entry("c2_dft_" + "x".join(map(str, dims)) + "_f64", ms, x.numel() * 32, err)
+        entry("c2_dft_" + "x".join(map(str, dims)) + "_f64", ms, x.numel() * 32, err,
+              cpu_baseline=cpu(["dft"], list(dims), 1, x.numel() * 32,
+                               "one N-D call, as the reference runs it (no parallelism in its N-D path)",
+                               threads=1, reps=2))
         del x, y
     # C2: Bluestein, N = 1,000,003 x 4
     n = 1000003
@@ -371,7 +419,10 @@ def bench_configs(args, stream):
         ms = timed(lambda: a.batched("dft", x, y, 4, n, n))
         torch.cuda.synchronize()
         err = rel(y[:1].cpu(), torch.fft.fft(x[:1], dim=1).cpu())
-    entry("c2_bluestein_dft_1000003x4_f64", ms, 4 * n * 32, err)
+    entry("c2_bluestein_dft_1000003x4_f64", ms, 4 * n * 32, err,
+          cpu_baseline=cpu(["dft"], [n], 4, 4 * n * 32,
+                           "4 transforms, OpenMP over the batch; scalar double build, the only reference build "
+                           "whose Bluestein output is correct", lib="libref_d_scalar.so", reps=2))
     del x, y
 
     # the batched c2c range of the FP64 roofline target: N = 2^12 .. 2^20, both
@@ -397,6 +448,9 @@ def bench_configs(args, stream):
     y = torch.empty_like(x)
     x64 = x[:64].to(torch.complex128)
     ref = torch.fft.fft(x64, dim=1)
+    c3_cpu = cpu(["dft"], [n], b, b * n * 16,
+                 f"{b} transforms, OpenMP over the batch; NOTORIOUS_FFT_SINGLE scalar build", lib="libref_s_scalar.so",
+                 prec="f32", reps=2)
     for name, form in (("fp32_plain", 0), ("split_tc", FORM_SPLIT_TC)):
         with Lf.mkaux("dft", [n]) as a:
             a.set_form(form)
@@ -405,11 +459,15 @@ def bench_configs(args, stream):
             d = (y[:64].to(torch.complex128) - ref)
             errs = torch.linalg.vector_norm(d, dim=1) / torch.linalg.vector_norm(ref, dim=1)
         entry(f"c3_{name}_65536x{b}_scaled10pct", ms, b * n * 16, float(errs.max().item()),
-              transforms_per_s=round(b / (ms * 1e-3), 1), scaled_in_sample=int((sel < 64).sum().item()))
+              transforms_per_s=round(b / (ms * 1e-3), 1), scaled_in_sample=int((sel < 64).sum().item()),
+              cpu_baseline=c3_cpu)
     del x, y, x64, ref
 
     # C4: ragged batch of 20,000 transforms, one persistent launch (CUDA graph)
     kinds, Ns = _uneven_config(20000, seed=2026)
+    listfile = tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False)
+    listfile.write("".join(f"{k} {nn}\n" for k, nn in zip(kinds, Ns)))
+    listfile.close()
     for L, tag, rs in ((Ld, "f64", 8), (Lf, "f32", 4)):
         t0 = time.perf_counter()
         bt = L.mkbatch(kinds, Ns)
@@ -441,9 +499,22 @@ def bench_configs(args, stream):
         err = rel(torch.complex(got[:, 0], got[:, 1]).cpu(), refc.cpu())
         info = bt.info()
         bt.free()
+        c4_cpu = None
+        if cpu_on:
+            lib = "libref_d_scalar.so" if rs == 8 else "libref_s_scalar.so"
+            rec = cpu_run(None, None, None, T, 2, lib=lib, prec=tag, listfile=listfile.name)
+            c4_cpu = cpu_entry(rec, rec["gbs"] * rec["seconds"] * 1e9 if rec else 0,
+                               "the same 20,000 (kind, N) list: one aux per distinct (kind, N), OpenMP over the "
+                               "groups, plan building excluded (seconds_with_plans includes it); the transforms "
+                               "the reference has no plan for (realdft / DCT-2 of lengths that are not powers "
+                               "of two) are not run and not counted", lib, T,
+                               extra=None if rec is None else {
+                                   "transforms_per_s": round(rec["transforms_per_s"], 1), "executed": rec["executed"],
+                                   "skipped_no_plan": rec["skipped_no_plan"],
+                                   "seconds_with_plans": round(rec["seconds_with_plans"], 3)})
         entry(f"c4_ragged_20000_{tag}", ms, nbytes, err, transforms_per_s=round(20000 / (ms * 1e-3), 1),
               build_s=round(build_s, 2), items=info["items"], tiles=info["tiles"], ctas=info["ctas"],
-              launches_per_call=1, graph=True)
+              launches_per_call=1, graph=True, cpu_baseline=c4_cpu)
         del xi, yo
 
     # C5: one forward + backward step of L = sum w |rfft2(x)|^2 + sum v DCT2(rowmean(x)), x 64 x 512 x 512 FP32
@@ -471,7 +542,11 @@ def bench_configs(args, stream):
     rf.free()
     dc.free()
     entry("c5_loss_forward_backward_64x512x512_f32", ms, 2 * (x.numel() * 4 + zz.numel() * 8), None,
-          note="realdft 2-D + DCT-2 forward, their adjoint kernels backward, torch elementwise glue")
+          note="realdft 2-D + DCT-2 forward, their adjoint kernels backward, torch elementwise glue",
+          cpu_baseline={"unavailable": "the reference's multi-dimensional realdft crashes (its N-D real path "
+                                       "dereferences a null scratch pointer; src/07_legacy.h:1492-1524) and it has "
+                                       "no adjoints"})
+    os.unlink(listfile.name)
     return out
 
 
@@ -648,12 +723,15 @@ def main():
 
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
-        threads = os.cpu_count() or 1
-        sample = max(threads * 2, 32) if N >= 65536 else 1024
-        s, kind = cpu_reference(["dft", "invdft"], N, sample, threads)
-        if s is not None:
-            cpu = {"value": round(2 * 2 * N * 16 / s / 1e9, 3), "unit": "GB/s", "cores": threads, "kind": kind,
-                   "sample": f"{sample} transforms of N={N} per direction, best of 3, OpenMP over the batch"}
+        # the reference's CPU path on the same workload: the whole batch,
+        # dft then invdft, best of 2 (about 1.5 s of 16-core work)
+        threads = host_cores()
+        rec = cpu_run(["dft", "invdft"], [N], B, threads, 2)
+        if rec is not None:
+            cpu = {"value": round(bytes_per_step / rec["seconds"] / 1e9, 3), "unit": "GB/s", "cores": threads,
+                   "cpu": cpu_model(), "kind": "reference", "ms_per_step": round(rec["seconds"] * 1e3, 2),
+                   "sample": f"the whole batch ({B} x dft then {B} x invdft in place, N={N}), best of 2, "
+                             f"OpenMP over the batch with one aux per thread, -O3 -fopenmp -mavx2 -mfma"}
     aux.free()
     if rank == 0:
         line = {

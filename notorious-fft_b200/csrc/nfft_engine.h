@@ -264,6 +264,10 @@ void note_launch();
 bool cluster_available(int logN);
 // Split-tensor-core pass (nfft_tc.cu, float library): LD_C / ST_C passes.
 bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStream_t s);
+// Radix-256 passes of the split tensor-core form (16-line tiles, persistent
+// CTAs, nfft_tc_lean.cuh); NOTORIOUS_FFT_TC_LEAN=0 selects tc_pass_kernel.
+bool tc_lean_enabled();
+bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s);
 int cluster_logr1(int logN);
 bool launch_cluster(const PassArgs& a1, const PassArgs& a2, int logN, long long ntransforms, cudaStream_t s);
 

@@ -455,7 +455,12 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
         rec->launches.push_back(r);
         return true;
     }
-    // split tensor-core form: radix-16 sub-stages on the tensor cores
+    // split tensor-core form: radix-256 passes in the specialized kernel, other
+    // radices with the radix-16 sub-stages of the generic pass on the tensor cores
+    if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR == 8 && tc_lean_enabled()) {
+        a.logJ = 4;
+        return launch_tc_lean(a, c->sm_count, s);
+    }
     if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR >= 4 && tile == 12 && logJ == 12 - logR) {
         a.logJ = logJ;
         long long nt = (a.nlines + (1ll << logJ) - 1) >> logJ;

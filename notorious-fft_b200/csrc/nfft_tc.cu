@@ -1,8 +1,18 @@
-// nfft_tc.cu -- the split-tensor-core pass kernel of the float library
-// (NOTORIOUS_FFT_FORM_SPLIT_TC): the generic Stockham pass (nfft_pass.cuh)
-// with its radix-16 sub-stages computed by tc_substage (nfft_tc.cuh).
+// nfft_tc.cu -- the split-tensor-core pass kernels of the float library
+// (NOTORIOUS_FFT_FORM_SPLIT_TC):
+//  * tc_lean_kernel: radix-256 passes, both radix-16 stages of a line as FP16
+//    hi + lo tensor-core products in registers (nfft_tc_lean.cuh), persistent
+//    CTAs over 16-line tiles -- every radix-256 pass of the form;
+//  * tc_pass_kernel: the generic Stockham pass (nfft_pass.cuh) with its
+//    radix-16 sub-stages computed by tc_substage (nfft_tc.cuh) -- the other
+//    pass radices.
+#include <stdlib.h>
+
+#include <algorithm>
+
 #include "nfft_engine.h"
 #include "nfft_tc.cuh"
+#include "nfft_tc_lean.cuh"
 
 namespace nfft {
 
@@ -72,6 +82,54 @@ __global__ void __launch_bounds__((1 << LOG_TILE) / 16) tc_pass_kernel(const Pas
     }
 }
 
+constexpr int TCL_THREADS = 256;
+
+// Persistent CTAs: the per-lane constants (F fragments, internal twiddles) are
+// set up once per CTA and reused for every tile it takes.
+__global__ void __launch_bounds__(TCL_THREADS, 2) tc_lean_kernel(const PassArgs a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    float2* sm = (float2*)smraw;
+    long long* lin = (long long*)(sm + TCL_SLOTS);
+    typename TcLean<TCL_THREADS>::Consts c;
+    TcLean<TCL_THREADS>::setup((const TwTables<float>*)a.tw, threadIdx.x & 31, c);
+    const long long ntiles = (a.nlines + TCL_J - 1) >> TCL_LOGJ;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        tc_lean_tile<TCL_THREADS>(a, c, tile, sm, lin);
+        __syncthreads();
+    }
+}
+
+bool tc_lean_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NOTORIOUS_FFT_TC_LEAN");
+        v = e ? atoi(e) : 1;
+    }
+    return v != 0;
+}
+
+bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s) {
+    static int per_sm = 0;
+    const size_t smem = tcl_smem_bytes<TCL_THREADS>();
+    if (!per_sm) {
+        if (!cuda_ok(cudaFuncSetAttribute((const void*)tc_lean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem),
+                     "cudaFuncSetAttribute(tc lean)"))
+            return false;
+        int n = 0;
+        if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tc_lean_kernel, TCL_THREADS, smem),
+                     "cudaOccupancyMaxActiveBlocksPerMultiprocessor(tc lean)"))
+            return false;
+        per_sm = n > 0 ? n : 1;
+    }
+    const long long ntiles = (a.nlines + TCL_J - 1) >> TCL_LOGJ;
+    if (ntiles <= 0) return true;
+    const long long grid = std::min<long long>(ntiles, (long long)std::max(sm_count, 1) * per_sm);
+    tc_lean_kernel<<<(unsigned)grid, TCL_THREADS, smem, s>>>(a);
+    note_launch();
+    return cuda_ok(cudaGetLastError(), "tensor-core radix-256 pass launch");
+}
+
 bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStream_t s) {
     static bool attr = false;
     const size_t smem = pass_smem_bytes<float>(log_tile);
@@ -93,6 +151,13 @@ bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStrea
 }
 
 #else
+
+bool tc_lean_enabled() { return false; }
+
+bool launch_tc_lean(const PassArgs&, int, cudaStream_t) {
+    set_error(6, "the split tensor-core form exists in the float library only");
+    return false;
+}
 
 bool launch_tc_pass(const PassArgs&, int, long long, cudaStream_t) {
     set_error(6, "the split tensor-core form exists in the float library only");

@@ -199,6 +199,7 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 #include "../../notorious-fft_b200/csrc/nfft_lean_list.h"
 #include "../../notorious-fft_b200/csrc/nfft_cluster.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_tc.cuh"
+#include "../../notorious-fft_b200/csrc/nfft_tc_lean.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_queue.h"
 #include "../../notorious-fft_b200/csrc/nfft_resident.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_resident_list.h"
@@ -782,6 +783,107 @@ bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStrea
             lns += lr;
         }
         for (int e = 0; e < E; ++e) store_slot<T, ST_C>(a, tw, sm.data(), tl, e);
+    }
+    return true;
+}
+
+// ---- radix-256 split tensor-core pass (nfft_tc_lean.cuh): the kernel's lane
+// phases for the 32 lanes of a warp around host models of its collectives (the
+// max reduction, and emu_mma for the FP16 hi / lo products).
+static void emu_tcl_stage(const TcA* A, uint32_t (*xb)[2][2][2][2], float (*acc)[2][2][4]) {
+    uint32_t a_h[32][4], a_l[32][4], b[32][2];
+    float d[32][4];
+    for (int nt = 0; nt < 2; ++nt)
+        for (int mt = 0; mt < 2; ++mt) {
+            for (int lane = 0; lane < 32; ++lane)
+                for (int i = 0; i < 4; ++i) d[lane][i] = 0.0f;
+            for (int kt = 0; kt < 2; ++kt) {
+                for (int lane = 0; lane < 32; ++lane) {
+                    const uint32_t* ah = mt == kt ? A[lane].rh : (mt == 0 ? A[lane].nih : A[lane].ih);
+                    const uint32_t* al = mt == kt ? A[lane].rl : (mt == 0 ? A[lane].nil : A[lane].il);
+                    for (int i = 0; i < 4; ++i) { a_h[lane][i] = ah[i]; a_l[lane][i] = al[i]; }
+                }
+                // Flo Xhi, Fhi Xlo, Fhi Xhi
+                for (int term = 0; term < 3; ++term) {
+                    const int hl = term == 1 ? 1 : 0;
+                    for (int lane = 0; lane < 32; ++lane)
+                        for (int r = 0; r < 2; ++r) b[lane][r] = xb[lane][kt][nt][hl][r];
+                    emu_mma(term == 0 ? a_l : a_h, b, d);
+                }
+            }
+            for (int lane = 0; lane < 32; ++lane)
+                for (int i = 0; i < 4; ++i) acc[lane][mt][nt][i] = d[lane][i];
+        }
+}
+
+bool tc_lean_enabled() {
+    const char* e = getenv("NOTORIOUS_FFT_TC_LEAN");
+    return !e || atoi(e) != 0;
+}
+
+bool launch_tc_lean(const PassArgs& a, int, cudaStream_t) {
+    if (sizeof(real_t) != 4) {
+        set_error(6, "the split tensor-core form exists in the float library only");
+        return false;
+    }
+    if constexpr (sizeof(real_t) == 4) {
+        using TL = TcLean<256>;
+        g_launches++;
+        const TwTables<float>* tw = (const TwTables<float>*)a.tw;
+        std::vector<TL::Consts> c(32);
+        TcA A[32];
+        for (int lane = 0; lane < 32; ++lane) {
+            TL::setup(tw, lane, c[lane]);
+            A[lane] = c[lane].A;
+        }
+        g_smem_elems = TCL_SLOTS;
+        std::vector<float2> sm(TCL_SLOTS);
+        long long lin[TCL_J], lout[TCL_J], lj[TCL_J];
+        TileLines tl{lin, lout, lj};
+        std::vector<TL::LineRegs> st(32);
+        uint32_t xb[32][2][2][2][2];
+        float acc[32][2][2][4];
+        const long long ntiles = (a.nlines + TCL_J - 1) >> TCL_LOGJ;
+        for (long long tile = 0; tile < ntiles; ++tile) {
+            for (auto& x : sm) x = make_float2(NAN, NAN);
+            for (int l = 0; l < TCL_J; ++l) line_setup(a, (tile << TCL_LOGJ) + l, l, tl);
+            for (int e = 0; e < TCL_SLOTS; ++e) {
+                int l, r;
+                tcl_walk(a.in_row, e, l, r);
+                float2 v = make_float2(0.f, 0.f);
+                if (lj[l] >= 0) {
+                    v = NFFT_GLD((const float2*)a.in + tcl_in_off(a, lin[l], lj[l], r));
+                    if (a.conj_in) v.y = -v.y;
+                }
+                sm[NFFT_SM(tcl_slot(r, l))] = v;
+            }
+            for (int l = 0; l < TCL_J; ++l) {
+                if (lj[l] < 0) continue;
+                float m = 0.f;
+                for (int lane = 0; lane < 32; ++lane) m = fmaxf(m, TL::load(a, tw, sm.data(), l, lj[l], lane, st[lane]));
+                for (int lane = 0; lane < 32; ++lane) {
+                    TL::split1(m, st[lane]);
+                    memcpy(xb[lane], st[lane].xb, sizeof xb[lane]);
+                }
+                emu_tcl_stage(A, xb, acc);
+                for (int lane = 0; lane < 32; ++lane) {
+                    memcpy(st[lane].acc, acc[lane], sizeof acc[lane]);
+                    TL::mid(c[lane], st[lane]);
+                    memcpy(xb[lane], st[lane].xb, sizeof xb[lane]);
+                }
+                emu_tcl_stage(A, xb, acc);
+                for (int lane = 0; lane < 32; ++lane) {
+                    memcpy(st[lane].acc, acc[lane], sizeof acc[lane]);
+                    TL::store(a, sm.data(), l, lane, st[lane]);
+                }
+            }
+            for (int e = 0; e < TCL_SLOTS; ++e) {
+                int l, r;
+                tcl_walk(a.out_row, e, l, r);
+                if (lj[l] < 0) continue;
+                NFFT_GST((float2*)a.out + tcl_out_off(a, lout[l], lj[l], r), sm[NFFT_SM(tcl_slot(r, l))]);
+            }
+        }
     }
     return true;
 }

@@ -329,3 +329,29 @@ print(float(np.linalg.norm(y - ref) / np.linalg.norm(ref)))
                        env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     assert float(r.stdout.strip().splitlines()[-1]) < 1e-13 * 17
+
+
+@pytest.mark.parametrize("n,batch", [(256, 5), (1 << 16, 3), (4096, 3)])
+@pytest.mark.parametrize("tc_lean", ["1", "0"])
+def test_emu_split_tc_form(emu_f, oracle_d, n, batch, tc_lean, monkeypatch):
+    """The split tensor-core form on the emulator (host model of the FP16
+    mma.sync fragments): radix-256 passes in the specialized kernel
+    (NOTORIOUS_FFT_TC_LEAN=1, 256 and 2^16) or all passes in the generic
+    tensor-core pass (=0; 4096 always), forward and inverse, one transform
+    scaled by 1e4 and one by 1e-4 -- every transform within 2e-6 of the
+    FP64 oracle."""
+    from notorious_fft import FORM_SPLIT_TC
+    monkeypatch.setenv("NOTORIOUS_FFT_TC_LEAN", tc_lean)
+    rng = np.random.default_rng(n + batch)
+    x = rng.standard_normal((batch, n)) + 1j * rng.standard_normal((batch, n))
+    x[0] *= 1e4
+    x[-1] *= 1e-4
+    x = x.astype(np.complex64)
+    with emu_f.mkaux("dft", [n]) as a:
+        a.set_form(FORM_SPLIT_TC)
+        for kind in ("dft", "invdft"):
+            y = np.zeros_like(x)
+            a.batched(kind, x, y, batch, n, n)
+            ref = oracle_d.transform(kind, x.astype(np.complex128))
+            errs = [rel_l2(y[b], ref[b]) for b in range(batch)]
+            assert max(errs) <= 2e-6, (kind, errs)
