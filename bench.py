@@ -74,10 +74,18 @@ class Clocks:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "25",
                                        "-i", str(index)], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        # wait (at most ~2 s) for the first sample, so the sampler is running
+        # when the timed region starts
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 2.0:
+            self.f.flush()
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.p is None:
@@ -645,6 +653,9 @@ def main():
         aux.batched("dft", x, y, B, N, N)
         aux.batched("invdft", y, z, B, N, N)
 
+    # clock samples: the sampler runs from before the warm-up steps (all under
+    # load) until the end of the timed region
+    clocks = Clocks(local)
     for _ in range(args.warmup):
         step()
         if flush is not None:
@@ -652,7 +663,6 @@ def main():
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    clocks = Clocks(local)
     times = []
     launches0 = L.launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)

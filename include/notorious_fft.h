@@ -265,11 +265,27 @@ int notorious_fft_batch_debug_withhold(notorious_fft_batch* b, long long spin_li
  * (kind, N) in the queue on this GPU, keeps the fastest, and stores it in the
  * tune cache (a JSON file: $NOTORIOUS_FFT_TUNE_CACHE, default
  * ~/.cache/notorious_fft/tune.json, keyed by GPU name + driver, precision,
- * kind and N).  Later batches use the cached split.  Returns 0 or an error. */
+ * kind and N).  Later batches use the cached split.  It then tunes standalone
+ * plans of the same length (see notorious_fft_tune_lookup_plan).  Returns 0
+ * or an error. */
 int notorious_fft_autotune(int kind, int N);
 /* The cached split for (kind, N): writes up to max_passes log2 radices and
  * returns their count (0: none cached). */
 int notorious_fft_tune_lookup(int kind, int N, int* log2_radices, int max_passes);
+/* notorious_fft_autotune also times standalone plans of the family of `kind`
+ * (the default schedule and the executable pass splits, each with the
+ * default thread rule and with 128- and 256-thread pass kernels) and caches
+ * the fastest; every later mkaux_* of that family uses the cached schedule
+ * for power-of-two axes of length N.  This returns the cached split (up to
+ * max_passes log2 radices; 0 = the default schedule) and writes the thread
+ * count (log2, 0 = the default rule) to *log2_threads; -1: nothing cached. */
+int notorious_fft_tune_lookup_plan(int kind, int N, int* log2_radices, int max_passes, int* log2_threads);
+/* The schedule an aux runs on one axis (0 = slowest, -1 = last): the pass
+ * radices (log2) of the axis's power-of-two inner FFT and the thread count
+ * (log2, 0 = the default rule) of its pass kernels.  Returns the pass count,
+ * 0 for a Bluestein axis, -1 on error. */
+int notorious_fft_aux_schedule(const notorious_fft_aux* a, int axis, int* log2_radices, int max_passes,
+                               int* log2_threads);
 
 /* Library identification: precision of this build's notorious_fft_real
  * (8 or 4) and a short version string. */

@@ -457,6 +457,38 @@ int notorious_fft_tune_lookup(int kind, int N, int* log2_radices, int max_passes
     return tune_lookup(kind, N, log2_radices, max_passes);
 }
 
+int notorious_fft_tune_lookup_plan(int kind, int N, int* log2_radices, int max_passes, int* log2_threads) {
+    clear_error();
+    int scratch[4];
+    if (!log2_radices || max_passes < 1) {
+        log2_radices = scratch;
+        max_passes = 4;
+    }
+    return tune_lookup_plan(kind, N, log2_radices, max_passes, log2_threads);
+}
+
+int notorious_fft_aux_schedule(const notorious_fft_aux* a, int axis, int* log2_radices, int max_passes,
+                               int* log2_threads) {
+    clear_error();
+    if (!a || !a->plan) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "NULL aux");
+        return -1;
+    }
+    const notorious_fft_plan* p = a->plan;
+    const int d = (int)p->axes.size();
+    if (axis < 0) axis += d;
+    if (axis < 0 || axis >= d) {
+        set_error(NOTORIOUS_FFT_ERR_INVALID, "axis %d out of range for a %d-dimensional aux", axis, d);
+        return -1;
+    }
+    const AxisPlan& ax = p->axes[axis];
+    if (!ax.pow2) return 0;
+    const FftSchedule& sch = ax.fft_contig;
+    for (int i = 0; i < sch.npass && log2_radices && i < max_passes; ++i) log2_radices[i] = sch.plog[i];
+    if (log2_threads) *log2_threads = sch.logt;
+    return sch.npass;
+}
+
 int notorious_fft_real_size(void) { return (int)sizeof(real_t); }
 long long notorious_fft_launch_count(void) { return launch_count(); }
 const char* notorious_fft_version(void) { return "notorious-fft-b200 0.1 (sm_100a)"; }

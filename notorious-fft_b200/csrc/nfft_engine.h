@@ -76,6 +76,7 @@ struct View {
 struct FftSchedule {
     int logL = 0;
     int npass = 0;
+    int logt = 0;                    // threads (log2) of the specialized pass kernels; 0: the default rule
     int plog[4] = {0, 0, 0, 0};      // pass radices (log2), in execution order
     int tile[4] = {12, 12, 12, 12};  // log2 tile size of each pass
     int nsub[4] = {0, 0, 0, 0};
@@ -167,6 +168,7 @@ struct OpSpec {
     bool paired = false;   // st is ST_R / ST_T2 (needs whole lines or the unpack epilogue)
     int vjp = 0;           // adjoint weights of the real operators
     int tc = 0;            // split tensor-core radix-16 sub-stages (float library)
+    int logt = 0;          // threads (log2) of the specialized pass kernels; 0: the default rule
     const void* post = nullptr;   // ST_BLUE_T2 post-twiddle table
 };
 
@@ -256,6 +258,18 @@ void batch_set_graph(notorious_fft_batch* b, int enable);
 void batch_withhold(notorious_fft_batch* b, long long spin_limit);
 int autotune(int kind, int n, cudaStream_t s);
 int tune_lookup(int kind, int n, int* plog, int max_passes);
+// Standalone plans: the cached pass split and thread count of a power-of-two
+// axis of transform family `family` and length n (false: none cached), and
+// the same for the C API.
+bool tune_get_plan(int family, int n, std::vector<int>& split, int& logt);
+int tune_lookup_plan(int kind, int n, int* plog, int max_passes, int* logt);
+// While set on the calling thread, build_axis uses this split / thread count
+// for every power-of-two axis instead of the cache (the autotuner's trials).
+struct PlanOverride {
+    std::vector<int> split;
+    int logt = 0;
+};
+PlanOverride*& plan_override();
 long long launch_count();
 void note_launch();
 

@@ -457,7 +457,7 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
     }
     // split tensor-core form: radix-256 passes in the specialized kernel, other
     // radices with the radix-16 sub-stages of the generic pass on the tensor cores
-    if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR == 8 && tc_lean_enabled()) {
+    if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR == 8 && logNs + 8 <= 24 && tc_lean_enabled()) {
         a.logJ = 4;
         return launch_tc_lean(a, c->sm_count, s);
     }
@@ -472,6 +472,7 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
         const bool rr = !ci && !co;
         int logT = (logR <= 12 && (rr || logR <= 10)) ? 8 : 9;
         if (lean_logt_pref(logL) == 7 && lean_available(logR, 7, ci, co, ldop, stop)) logT = 7;
+        if (op.logt && lean_available(logR, op.logt, ci, co, ldop, stop)) logT = op.logt;   // tuned
         if (lean_available(logR, logT, ci, co, ldop, stop)) {
             a.logJ = logT + 4 - logR;
             long long nt = (a.nlines + (1ll << a.logJ) - 1) >> a.logJ;
@@ -547,7 +548,9 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
         return launch_cluster(a1, a2, logL, src.nb ? src.cnt[0] : 1, s);
     }
     if (np == 1 && !(op.paired && strided)) {
-        return run_pass(c, src, dst, logL, 0, sch.plog[0], sch.tile[0], sch.nsub[0], sch.sub[0], op, true, true, 0, 0,
+        OpSpec o1 = op;
+        o1.logt = sch.logt;
+        return run_pass(c, src, dst, logL, 0, sch.plog[0], sch.tile[0], sch.nsub[0], sch.sub[0], o1, true, true, 0, 0,
                         nullptr, nullptr, s);
     }
     // multi-pass (or a paired op on strided lines): chunk the outermost batch dim
@@ -629,6 +632,7 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
             if (to_user) out = vd;
             else out = scratch_view(buf[i % nbuf], vs, L, strided && !paired_epilogue);
             OpSpec o = op;
+            o.logt = sch.logt;
             if (last && paired_epilogue) {
                 o.st = ST_C;
                 o.scale = 1.0;
@@ -795,6 +799,11 @@ static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const 
 // ---------------------------------------------------------------------------
 // plans
 // ---------------------------------------------------------------------------
+PlanOverride*& plan_override() {
+    thread_local PlanOverride* o = nullptr;
+    return o;
+}
+
 static bool build_axis(notorious_fft_plan* p, const DeviceCtx* c, AxisPlan& ax, int n, int family, int max_tile = 13) {
     ax.n = n;
     ax.pow2 = is_pow2(n);
@@ -803,6 +812,28 @@ static bool build_axis(notorious_fft_plan* p, const DeviceCtx* c, AxisPlan& ax, 
         int logL = (family == FAM_DFT) ? ax.logn : std::max(0, ax.logn - 1);
         ax.fft_contig = make_schedule(logL, false, max_tile);
         ax.fft_strided = make_schedule(logL, true, max_tile);
+        // standalone plans: an autotuner trial, else the tune cache's split and
+        // thread count for (family, n) on this GPU (a split this build cannot
+        // run keeps the default schedule)
+        if (!recorder() && logL >= 1) {
+            std::vector<int> split;
+            int logt = 0;
+            bool have = false;
+            if (PlanOverride* o = plan_override()) {
+                split = o->split;
+                logt = o->logt;
+                have = true;
+            } else {
+                have = tune_get_plan(family, n, split, logt);
+            }
+            if (have) {
+                FftSchedule t;
+                if (split.empty()) t = ax.fft_contig;
+                else if (!make_split_schedule(logL, split.data(), (int)split.size(), &t)) t = ax.fft_contig;
+                t.logt = (logt == 7 || logt == 8 || logt == 9) ? logt : 0;
+                ax.fft_contig = t;
+            }
+        }
         return true;
     }
     if (family != FAM_DFT) {

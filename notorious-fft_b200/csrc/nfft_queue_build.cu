@@ -582,6 +582,7 @@ namespace {
 std::mutex g_tune_mu;
 bool g_tune_loaded = false;
 std::map<std::string, std::vector<int>> g_tune;   // key -> split
+std::map<std::string, int> g_tune_logt;           // key -> threads (log2) of standalone plans, 0: default
 std::map<std::string, std::string> g_tune_lines;  // key -> file line of this device (kept on save)
 std::vector<std::string> g_tune_foreign;          // lines of other devices (kept verbatim)
 
@@ -608,6 +609,20 @@ std::string device_tag() {
 
 std::string tune_key(int kind, int n) {
     return std::string(sizeof(real_t) == 8 ? "f64:" : "f32:") + kind_name(kind) + ":" + std::to_string(n);
+}
+
+// Standalone plans are keyed by transform family: the inner FFT schedule of a
+// power-of-two axis is shared by the kinds of a family.
+const char* family_name(int fam) {
+    switch (fam) {
+    case FAM_DFT: return "dft";
+    case FAM_REAL: return "realdft";
+    case FAM_T2T3: return "t2t3";
+    default: return "t4";
+    }
+}
+std::string tune_key_plan(int fam, int n) {
+    return std::string(sizeof(real_t) == 8 ? "f64:plan:" : "f32:plan:") + family_name(fam) + ":" + std::to_string(n);
 }
 
 // The string value of "name": "..." in line, or "".
@@ -648,9 +663,14 @@ void tune_load_locked() {
             s = end;
             while (*s == ',' || *s == ' ') ++s;
         }
-        if (!split.empty()) {
+        // plan entries may carry an empty split (the default schedule) and a
+        // thread count; queue entries always name a split
+        const bool plan = key.find(":plan:") != std::string::npos;
+        if (!split.empty() || plan) {
             g_tune[key] = split;
             g_tune_lines[key] = line;
+            size_t q = line.find("\"logt\": ");
+            g_tune_logt[key] = q == std::string::npos ? 0 : atoi(line.c_str() + q + 8);
         }
     }
     fclose(f);
@@ -690,6 +710,33 @@ bool tune_get(int kind, int n, std::vector<int>& split) {
     return true;
 }
 
+bool tune_get_plan(int fam, int n, std::vector<int>& split, int& logt) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
+    const std::string key = tune_key_plan(fam, n);
+    auto it = g_tune.find(key);
+    if (it == g_tune.end()) return false;
+    split = it->second;
+    auto lt = g_tune_logt.find(key);
+    logt = lt == g_tune_logt.end() ? 0 : lt->second;
+    return true;
+}
+
+static void tune_put_plan(int fam, int n, const std::vector<int>& split, int logt, double us) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
+    const std::string key = tune_key_plan(fam, n);
+    std::string sp;
+    for (size_t i = 0; i < split.size(); ++i) sp += (i ? ", " : "") + std::to_string(split[i]);
+    char buf[768];
+    snprintf(buf, sizeof buf, "{\"device\": \"%s\", \"key\": \"%s\", \"split\": [%s], \"logt\": %d, \"us\": %.2f}",
+             device_tag().c_str(), key.c_str(), sp.c_str(), logt, us);
+    g_tune[key] = split;
+    g_tune_logt[key] = logt;
+    g_tune_lines[key] = buf;
+    tune_save_locked();
+}
+
 static void tune_put(int kind, int n, const std::vector<int>& split, double us) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     tune_load_locked();
@@ -721,6 +768,92 @@ static std::vector<std::vector<int>> tune_candidates(int logL) {
     });
     if (c.size() > 5) c.resize(5);
     return c;
+}
+
+// Standalone plans of (family of kind, n): time the default schedule and the
+// executable pass splits, each with the default thread rule and with 128- and
+// 256-thread pass kernels, on a ~256 MB batch of `kind`; store the fastest.
+static int autotune_plan(int kind, int n, cudaStream_t s) {
+    const int fam = family_of(kind);
+    int logn = 0;
+    while ((1 << logn) < n) ++logn;
+    const int logL = fam == FAM_DFT ? logn : logn - 1;
+    std::vector<std::vector<int>> splits = {{}};   // {} = the default schedule
+    for (auto& c : tune_candidates(logL))
+        if (!c.empty()) splits.push_back(c);
+    const int logts[3] = {0, 7, 8};
+    const long long bytes = (in_reals_of(kind, n) + out_reals_of(kind, n)) * (long long)sizeof(real_t);
+    const long long cnt = std::max(1ll, (256ll << 20) / bytes);
+    void *din = nullptr, *dout = nullptr;
+    const size_t ib = (size_t)cnt * (size_t)in_reals_of(kind, n) * sizeof(real_t);
+    const size_t ob = (size_t)cnt * (size_t)out_reals_of(kind, n) * sizeof(real_t);
+    if (!cuda_ok(cudaMalloc(&din, ib), "cudaMalloc(tune input)")) return last_error();
+    if (!cuda_ok(cudaMalloc(&dout, ob), "cudaMalloc(tune output)")) {
+        cudaFree(din);
+        return last_error();
+    }
+    cudaMemsetAsync(din, 0, ib, s);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e30;
+    std::vector<int> best_split;
+    int best_logt = 0, rc = 0;
+    for (auto& split : splits) {
+        for (int lt : logts) {
+            PlanOverride o;
+            o.split = split;
+            o.logt = lt;
+            plan_override() = &o;
+            notorious_fft_plan* p = plan_create(fam, 1, &n);
+            plan_override() = nullptr;
+            if (!p) {
+                clear_error();
+                continue;
+            }
+            const long long ie = plan_in_elems(p, kind), oe = plan_out_elems(p, kind);
+            std::vector<float> ms;
+            bool ok = true;
+            for (int it = 0; it < 7 && ok; ++it) {
+                cudaEventRecord(e0, s);
+                ok = plan_execute(p, kind, din, dout, cnt, ie, oe, s, 0) == 0;
+                cudaEventRecord(e1, s);
+                ok = ok && cuda_ok(cudaEventSynchronize(e1), "tune timing");
+                float t = 0;
+                cudaEventElapsedTime(&t, e0, e1);
+                if (it >= 2) ms.push_back(t);
+            }
+            plan_destroy(p);
+            if (!ok) {
+                rc = last_error() ? last_error() : 4;
+                break;
+            }
+            std::sort(ms.begin(), ms.end());
+            const double med = ms.empty() ? 1e30 : ms[ms.size() / 2];
+            if (med < best) {
+                best = med;
+                best_split = split;
+                best_logt = lt;
+            }
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(din);
+    cudaFree(dout);
+    if (rc) return rc;
+    if (best < 1e30) tune_put_plan(fam, n, best_split, best_logt, best * 1000.0 / (double)cnt);
+    return 0;
+}
+
+int tune_lookup_plan(int kind, int n, int* plog, int max_passes, int* logt) {
+    std::vector<int> split;
+    int lt = 0;
+    if (kind < 0 || kind > 9 || !tune_get_plan(family_of(kind), n, split, lt)) return -1;
+    for (int i = 0; i < (int)split.size() && i < max_passes; ++i) plog[i] = split[i];
+    if (logt) *logt = lt;
+    return (int)split.size();
 }
 
 int autotune(int kind, int n, cudaStream_t s) {
@@ -788,12 +921,9 @@ int autotune(int kind, int n, cudaStream_t s) {
     cudaFree(din);
     cudaFree(dout);
     if (rc) return rc;
-    if (best_split.empty()) {
-        // only the default schedule was executable
-        return 0;
-    }
-    tune_put(kind, n, best_split, best * 1000.0 / (double)cnt);
-    return 0;
+    if (!best_split.empty()) tune_put(kind, n, best_split, best * 1000.0 / (double)cnt);
+    // (the queue has no other choice than the default schedule otherwise)
+    return autotune_plan(kind, n, s);
 }
 
 int tune_lookup(int kind, int n, int* plog, int max_passes) {

@@ -85,18 +85,47 @@ __global__ void __launch_bounds__((1 << LOG_TILE) / 16) tc_pass_kernel(const Pas
 constexpr int TCL_THREADS = 256;
 
 // Persistent CTAs: the per-lane constants (F fragments, internal twiddles) are
-// set up once per CTA and reused for every tile it takes.
-__global__ void __launch_bounds__(TCL_THREADS, 2) tc_lean_kernel(const PassArgs a) {
+// set up once per CTA and reused for every tile it takes; the copies of the
+// next tile overlap the transform and the write-out of the current one.
+template <int MINB>
+__global__ void __launch_bounds__(TCL_THREADS, MINB) tc_lean_kernel(const PassArgs a) {
+    using P = TcPipe<TCL_THREADS>;
+    using TL = TcLean<TCL_THREADS>;
     extern __shared__ __align__(16) unsigned char smraw[];
-    float2* sm = (float2*)smraw;
-    long long* lin = (long long*)(sm + TCL_SLOTS);
-    typename TcLean<TCL_THREADS>::Consts c;
-    TcLean<TCL_THREADS>::setup((const TwTables<float>*)a.tw, threadIdx.x & 31, c);
+    float2* const buf0 = (float2*)smraw;                              // buffers: buf0 + b TCL_SLOTS
+    long long* const lb0 = (long long*)(buf0 + 2 * TCL_SLOTS);        // line offsets: lb0 + b 3 TCL_J
+    typename TL::Consts* const tab = (typename TL::Consts*)(lb0 + 6 * TCL_J);
+    auto buf = [&](int b) { return buf0 + b * TCL_SLOTS; };
+    auto lb = [&](int b) { return lb0 + b * 3 * TCL_J; };
+    if (threadIdx.x < 32) TL::setup((const TwTables<float>*)a.tw, threadIdx.x, tab[threadIdx.x]);
+    const typename TL::Consts& c = tab[threadIdx.x & 31];
+    uint64_t pol_in, pol_out;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_in));
+    if (a.hint_out >= 2) asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol_out));
+    else asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_out));
     const long long ntiles = (a.nlines + TCL_J - 1) >> TCL_LOGJ;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        tc_lean_tile<TCL_THREADS>(a, c, tile, sm, lin);
+    long long tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    P::lines(a, tile, lb(0));
+    __syncthreads();
+    P::prefetch(a, lb(0), buf(0), pol_in);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int k = 0; tile < ntiles; tile += gridDim.x, ++k) {
+        const int cur = k & 1, nxt = cur ^ 1;
+        const long long next = tile + gridDim.x;
+        // the buffer and line offsets of `nxt` were last read before the
+        // barrier that ended the previous write-out
+        if (next < ntiles) P::lines(a, next, lb(nxt));
         __syncthreads();
+        if (next < ntiles) P::prefetch(a, lb(nxt), buf(nxt), pol_in);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+        P::compute(a, c, lb(cur), buf(cur));
+        __syncthreads();
+        P::writeout(a, lb(cur), buf(cur), pol_out);
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 bool tc_lean_enabled() {
@@ -108,16 +137,29 @@ bool tc_lean_enabled() {
     return v != 0;
 }
 
+// CTAs per SM the kernel is compiled for: 2 (default, 128 registers) or 3
+// (NOTORIOUS_FFT_TC_CTAS=3: 80 registers with a few spills; measured slower
+// on B200, 1339 vs 1552 GB/s on 2^16 x 2048).
+static int tc_lean_ctas() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NOTORIOUS_FFT_TC_CTAS");
+        v = (e && atoi(e) == 3) ? 3 : 2;
+    }
+    return v;
+}
+
 bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s) {
     static int per_sm = 0;
+    const int minb = tc_lean_ctas();
+    const void* fn = minb == 2 ? (const void*)tc_lean_kernel<2> : (const void*)tc_lean_kernel<3>;
     const size_t smem = tcl_smem_bytes<TCL_THREADS>();
     if (!per_sm) {
-        if (!cuda_ok(cudaFuncSetAttribute((const void*)tc_lean_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem),
+        if (!cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                      "cudaFuncSetAttribute(tc lean)"))
             return false;
         int n = 0;
-        if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tc_lean_kernel, TCL_THREADS, smem),
+        if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, TCL_THREADS, smem),
                      "cudaOccupancyMaxActiveBlocksPerMultiprocessor(tc lean)"))
             return false;
         per_sm = n > 0 ? n : 1;
@@ -125,7 +167,8 @@ bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s) {
     const long long ntiles = (a.nlines + TCL_J - 1) >> TCL_LOGJ;
     if (ntiles <= 0) return true;
     const long long grid = std::min<long long>(ntiles, (long long)std::max(sm_count, 1) * per_sm);
-    tc_lean_kernel<<<(unsigned)grid, TCL_THREADS, smem, s>>>(a);
+    if (minb == 2) tc_lean_kernel<2><<<(unsigned)grid, TCL_THREADS, smem, s>>>(a);
+    else tc_lean_kernel<3><<<(unsigned)grid, TCL_THREADS, smem, s>>>(a);
     note_launch();
     return cuda_ok(cudaGetLastError(), "tensor-core radix-256 pass launch");
 }

@@ -26,7 +26,7 @@
 namespace nfft {
 
 // Per-lane A fragments of F16: real / imaginary parts, hi / lo, and -Fi.
-struct TcA {
+struct __align__(16) TcA {
     uint32_t rh[4], rl[4], ih[4], il[4], nih[4], nil[4];
 };
 

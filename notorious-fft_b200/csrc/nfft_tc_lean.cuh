@@ -46,6 +46,7 @@
 #pragma once
 
 #include <cuda_fp16.h>
+#include <string.h>
 
 #include "nfft_tc.cuh"
 
@@ -62,9 +63,12 @@ NFFT_HD int tcl_slot(int r, int l) {
     return (r << TCL_LOGJ) | (l ^ s);
 }
 
+// Two tile buffers, two sets of line offsets, and the per-lane constants
+// (F fragments and internal twiddles, 32 lanes; see TcLean::Consts).
+constexpr size_t TCL_CONSTS_BYTES = 32 * 256;
 template <int THREADS>
 constexpr size_t tcl_smem_bytes() {
-    return sizeof(float2) * (size_t)TCL_SLOTS + sizeof(long long) * 3 * (size_t)TCL_J;
+    return 2 * (sizeof(float2) * (size_t)TCL_SLOTS + sizeof(long long) * 3 * (size_t)TCL_J) + TCL_CONSTS_BYTES;
 }
 
 NFFT_HD uint32_t tcl_pack(float lo16, float hi16) {
@@ -102,37 +106,90 @@ NFFT_HD void tcl_mma(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
     (void)d; (void)a; (void)b0; (void)b1;
 #endif
 }
+// d = a b (zero accumulator)
+NFFT_HD void tcl_mma0(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
+#if defined(__CUDA_ARCH__)
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%10, %10, %10, %10};"
+        : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(0.0f));
+#else
+    (void)a; (void)b0; (void)b1;
+    d[0] = d[1] = d[2] = d[3] = 0.0f;
+#endif
+}
 
-// One complex 16 x 16 product on the tensor cores: acc[mt][nt][i] =
-// ([[Fr, -Fi], [Fi, Fr]] [Xr; Xi]) with B fragments xb[kt][nt][hi/lo][reg];
-// the three terms of each block with the small ones first.
-NFFT_HD void tcl_terms(float* d, const uint32_t* ah, const uint32_t* al, const uint32_t (&x)[2][2]) {
-    tcl_mma(d, al, x[0][0], x[0][1]);
+// The three terms of block (ah, al) times x (small ones first), into d.
+NFFT_HD void tcl_terms(float* d, const uint32_t* ah, const uint32_t* al, const uint32_t (&x)[2][2], bool first) {
+    if (first) tcl_mma0(d, al, x[0][0], x[0][1]);
+    else tcl_mma(d, al, x[0][0], x[0][1]);
     tcl_mma(d, ah, x[1][0], x[1][1]);
     tcl_mma(d, ah, x[0][0], x[0][1]);
 }
+// One complex 16 x 16 product on the tensor cores: acc[mt][nt][i] =
+// ([[Fr, -Fi], [Fi, Fr]] [Xr; Xi]) with B fragments xb[kt][nt][hi/lo][reg],
+// walking the A blocks (Fr, then -Fi, then Fi) so that each is read once.
 NFFT_HD void tcl_stage(const TcA& A, const uint32_t (&xb)[2][2][2][2], float (&acc)[2][2][4]) {
+    {
+        uint32_t h[4], l[4];
 #pragma unroll
-    for (int nt = 0; nt < 2; ++nt) {
+        for (int i = 0; i < 4; ++i) { h[i] = A.rh[i]; l[i] = A.rl[i]; }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) acc[0][nt][i] = acc[1][nt][i] = 0.0f;
-        tcl_terms(acc[0][nt], A.rh, A.rl, xb[0][nt]);     // Yr += Fr Xr
-        tcl_terms(acc[0][nt], A.nih, A.nil, xb[1][nt]);   // Yr -= Fi Xi
-        tcl_terms(acc[1][nt], A.ih, A.il, xb[0][nt]);     // Yi += Fi Xr
-        tcl_terms(acc[1][nt], A.rh, A.rl, xb[1][nt]);     // Yi += Fr Xi
+        for (int nt = 0; nt < 2; ++nt) {
+            tcl_terms(acc[0][nt], h, l, xb[0][nt], true);    // Yr  = Fr Xr
+            tcl_terms(acc[1][nt], h, l, xb[1][nt], true);    // Yi  = Fr Xi
+        }
+    }
+    {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { h[i] = A.nih[i]; l[i] = A.nil[i]; }
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) tcl_terms(acc[0][nt], h, l, xb[1][nt], false);   // Yr -= Fi Xi
+    }
+    {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { h[i] = A.ih[i]; l[i] = A.il[i]; }
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) tcl_terms(acc[1][nt], h, l, xb[0][nt], false);   // Yi += Fi Xr
     }
 }
 
-// Exponent e with m 2^e in [2^9, 2^10) (m > 0), clamped to keep 2^e and
-// 2^-e normal; 0 for m = 0 or non-finite m.
+// W_{2^logP}^q for logP <= 24 from two table levels, without branches
+// (T1[0] = 1 exactly): every lane of a warp takes the same path.
+template <typename T>
+NFFT_HD C2<T> tcl_twiddle(const TwTables<T>* tw, uint64_t q, int logP) {
+    const uint64_t u = (q << (36 - logP)) & ((1ull << 36) - 1);
+    return cmul(tw_load<T>(tw, 0, (uint32_t)(u >> 24)), tw_load<T>(tw, 1, (uint32_t)(u >> 12) & (TW_SIZE - 1)));
+}
+
+// Exponent s with m 2^s in [2^9, 2^10) for the largest component m of a line,
+// read from the bits of m; 0 for m = 0, non-finite m or a subnormal m (a line
+// that small is below any rounding level of the transform).
 NFFT_HD int tcl_scale_exp(float m) {
-    if (!(m > 0.0f) || !(m < 3.0e38f)) return 0;
-    int e;
-    frexpf(m, &e);   // m = f 2^e, f in [0.5, 1)
-    int s = 10 - e;
-    if (s > 120) s = 120;
-    if (s < -120) s = -120;
-    return s;
+#if defined(__CUDA_ARCH__)
+    const int bits = __float_as_int(m);
+#else
+    int bits;
+    memcpy(&bits, &m, sizeof bits);
+#endif
+    const int em = (bits >> 23) & 0xff;   // m in [2^(em-127), 2^(em-126))
+    if (em == 0 || em == 255) return 0;
+    int s = 136 - em;
+    return s > 120 ? 120 : (s < -120 ? -120 : s);
+}
+// 2^s for |s| <= 126, exactly.
+NFFT_HD float tcl_pow2(int s) {
+    const int bits = (127 + s) << 23;
+#if defined(__CUDA_ARCH__)
+    return __int_as_float(bits);
+#else
+    float f;
+    memcpy(&f, &bits, sizeof f);
+    return f;
+#endif
 }
 
 // Tile slot e (0 <= e < 16 x 256) of a load or store walk -> (line l, point r):
@@ -153,6 +210,22 @@ NFFT_HD long long tcl_out_off(const PassArgs& a, long long bout, long long j, in
     return bout + base * a.out_estride + (long long)r * (a.out_estride << logNso);
 }
 
+// p[off] for p pointing into the shared tile sm (the emulator checks the
+// absolute slot (p - sm) + off).
+template <typename V>
+NFFT_HD V& tcl_at(V* sm, V* p, int off) {
+    (void)NFFT_SM((int)(p - sm) + off);
+    return p[off];
+}
+template <typename V>
+NFFT_HD const V& tcl_at(const V* sm, const V* p, int off) {
+    (void)NFFT_SM((int)(p - sm) + off);
+    return p[off];
+}
+
+// Swizzle of tile row r (see tcl_slot).
+NFFT_HD int tcl_swz(int r) { return ((r ^ (r >> 4)) & 1) | (r & 6) | ((((r >> 5) ^ (r >> 3)) & 1) << 3); }
+
 template <int THREADS>
 struct TcLean {
     static constexpr int WARPS = THREADS / 32;
@@ -162,10 +235,13 @@ struct TcLean {
 
     // Per-lane constants: F fragments and the internal twiddles W_256^{b k1}
     // of the lane's stage-1 outputs (k1 = g + 8 (i >> 1), b = 2q + (i & 1) + 8 nt).
-    struct Consts {
+    // The kernel keeps them in shared memory (one copy per CTA, read where
+    // used), which leaves registers for a third CTA per SM.
+    struct __align__(16) Consts {
         TcA A;
         float2 itw[2][4];
     };
+    static_assert(32 * sizeof(Consts) <= TCL_CONSTS_BYTES, "constants table");
 
     static NFFT_HD void setup(const TwTables<float>* tw, int lane, Consts& c) {
         tc_make_A(lane, c.A);
@@ -202,41 +278,66 @@ struct TcLean {
         int e;                     // scale exponent of the line
     };
 
-    // Phase 1: the lane's 8 points from shared memory, pass pre-twiddle
+    // Shared slots of the lane's fragment points on line l.  With the bits of
+    // r_in = b + 16 a (g: bits 0-2, nt: 3, h: 4, q: 5-6, i: 7) the swizzle is
+    // S = g ^ h ^ ((nt ^ q0) << 3), so slot = ((g + 32 q) << 4) + (l ^ g ^ (q0 << 3))
+    // ^ (h | nt << 3), plus the compile-time row offset ((8 nt + 16 h + 128 i) << 4).
+    // Coming out, r_out = k1 + 16 k2 has (i & 1): bit 0, q: 1-2, nt: 3, g: 4-6,
+    // i >> 1: 7, so S = (i & 1) ^ g0 ^ (q << 1) ^ ((nt ^ g1) << 3).
+    static NFFT_HD int in_slot(int lane, int l, int nt, int i, int h) {
+        const int g = lane >> 2, q = lane & 3;
+        return (((g + 32 * q) << 4) + (((8 * nt + 16 * h + 128 * i)) << 4)) +
+               ((l ^ g ^ ((q & 1) << 3)) ^ (h | (nt << 3)));
+    }
+    static NFFT_HD int out_slot(int lane, int l, int nt, int i) {
+        const int g = lane >> 2, q = lane & 3;
+        return (((2 * q + 16 * g) << 4) + (((i & 1) + 8 * nt + 128 * (i >> 1)) << 4)) +
+               ((l ^ (g & 1) ^ (q << 1) ^ (((g >> 1) & 1) << 3)) ^ ((i & 1) | (nt << 3)));
+    }
+
+    // Phase 1: the lane's 8 points from shared memory (conjugated for an
+    // inverse transform's first pass), pass pre-twiddle
     // W_{Ns R}^{r k} (k = j mod Ns, r = b + 16 a: W^{b k} per butterfly times
     // (W^{16 k})^a per point).  Returns the lane's largest component.
     static NFFT_HD float load(const PassArgs& a, const TwTables<float>* tw, const float2* sm, int l, long long j,
                               int lane, LineRegs& s) {
+        // slot = base + (lx ^ (h | nt << 3)) + ((8 nt + 16 h + 128 i) << 4): four
+        // base pointers per line, the rest compile-time offsets
+        const int g = lane >> 2, q = lane & 3;
+        const float2* base = sm + ((g + 32 * q) << 4);
+        const int lx = l ^ g ^ ((q & 1) << 3);
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
+            for (int h = 0; h < 2; ++h) {
+                const float2* p = base + (lx ^ (h | (nt << 3)));
 #pragma unroll
-                for (int h = 0; h < 2; ++h) s.x[nt][i][h] = sm[NFFT_SM(tcl_slot(in_point(lane, nt, i, h), l))];
-        if (a.logNs > 0) {
-            const long long k = j & ((1ll << a.logNs) - 1);
-            if (k) {
-                const int g = lane >> 2, q = lane & 3;
-                const int logP = a.logNs + TCL_LOGR;
-                const float2 wb0 = twiddle<float>(tw, (uint64_t)g * (uint64_t)k, logP);
-                const float2 w8 = twiddle<float>(tw, (uint64_t)8 * (uint64_t)k, logP);
-                const float2 wb1 = cmul(wb0, w8);
-                const float2 s1 = twiddle<float>(tw, (uint64_t)16 * (uint64_t)k, logP);
-                const float2 va = twiddle<float>(tw, (uint64_t)(32 * q) * (uint64_t)k, logP);
-                const float2 s8 = twiddle<float>(tw, (uint64_t)128 * (uint64_t)k, logP);
-                float2 v[2][2];
-                v[0][0] = va;
-                v[0][1] = cmul(va, s1);
-                v[1][0] = cmul(va, s8);
-                v[1][1] = cmul(v[1][0], s1);
+                for (int i = 0; i < 2; ++i) s.x[nt][i][h] = tcl_at(sm, p, (8 * nt + 16 * h + 128 * i) << 4);
+            }
+        if (a.conj_in) {
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
                 for (int i = 0; i < 2; ++i)
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        s.x[0][i][h] = cmul(s.x[0][i][h], cmul(wb0, v[i][h]));
-                        s.x[1][i][h] = cmul(s.x[1][i][h], cmul(wb1, v[i][h]));
-                    }
-            }
+                    for (int h = 0; h < 2; ++h) s.x[nt][i][h].y = -s.x[nt][i][h].y;
+        }
+        if (a.logNs > 0) {
+            // the per-point factor (W_P^{16 k})^a = W_{P/16}^{a k} (P = Ns R);
+            // the per-butterfly factor W_P^{b k} joins the internal twiddle (mid).
+            // k < 2^logNs <= 2^16 and a < 16: 32-bit products.
+            const uint32_t k = (uint32_t)j & ((1u << a.logNs) - 1);
+            const int logQ = a.logNs + 4;
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t e = (uint32_t)(2 * q + 8 * i + h) * k;
+                    const float2 v = logQ <= TW_BITS ? twiddle_small<float>(tw, e, logQ)
+                                                     : tcl_twiddle<float>(tw, (uint64_t)e, logQ);
+                    s.x[0][i][h] = cmul(s.x[0][i][h], v);
+                    s.x[1][i][h] = cmul(s.x[1][i][h], v);
+                }
         }
         float m = 0.0f;
 #pragma unroll
@@ -248,30 +349,64 @@ struct TcLean {
         return m;
     }
 
-    // Phase 2: scale by the line's power of two (m = the line's largest
-    // component) and split into stage 1's B fragments.
+    // Phase 2: the line's power-of-two scale (m = its largest component) and
+    // the split into stage 1's B fragments.  A line whose largest component
+    // is already in [1, 2^10) is not scaled: FP16 holds its stage-1 outputs
+    // (< 16 sqrt(2) 2^10) and the lo parts keep an absolute floor of 2^-25,
+    // far below such a line's rounding level.
     static NFFT_HD void split1(float m, LineRegs& s) {
-        s.e = tcl_scale_exp(m);
-        const float sc = ldexpf(1.0f, s.e);
+        s.e = (m >= 1.0f && m < 1024.0f) ? 0 : tcl_scale_exp(m);
+        if (s.e != 0) {
+            const float sc = tcl_pow2(s.e);
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) s.x[nt][i][h] = mkc(s.x[nt][i][h].x * sc, s.x[nt][i][h].y * sc);
+        }
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
-                tcl_split2(s.x[nt][i][0].x * sc, s.x[nt][i][1].x * sc, s.xb[0][nt][0][i], s.xb[0][nt][1][i]);
-                tcl_split2(s.x[nt][i][0].y * sc, s.x[nt][i][1].y * sc, s.xb[1][nt][0][i], s.xb[1][nt][1][i]);
+                tcl_split2(s.x[nt][i][0].x, s.x[nt][i][1].x, s.xb[0][nt][0][i], s.xb[0][nt][1][i]);
+                tcl_split2(s.x[nt][i][0].y, s.x[nt][i][1].y, s.xb[1][nt][0][i], s.xb[1][nt][1][i]);
             }
     }
 
-    // Phase 3: internal twiddle W_256^{b k1} on the stage-1 accumulators, then
+    // Phase 3: the twiddle of the stage-1 accumulators, W_256^{b k1} times,
+    // after the first pass, the per-butterfly part W_P^{b k} of the pass
+    // pre-twiddle (k = j mod Ns, P = Ns R; b = 2q + (i & 1) + 8 nt here), then
     // stage 2's B fragments: B2[kt][nt2] reg 0 = (b = 2q, 2q+1) from n-tile 0,
     // reg 1 = (b = 2q+8, 2q+9) from n-tile 1, both at k1 = g + 8 nt2
     // (accumulator regs 2 nt2 + {0, 1}).
-    static NFFT_HD void mid(const Consts& c, LineRegs& s) {
+    static NFFT_HD void mid(const PassArgs& a, const TwTables<float>* tw, const Consts& c, long long j, int lane,
+                            LineRegs& s) {
+        float2 t[2][4];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) t[nt][i] = c.itw[nt][i];
+        if (a.logNs > 0) {
+            const uint32_t k = (uint32_t)j & ((1u << a.logNs) - 1);
+            const int logP = a.logNs + TCL_LOGR, q = lane & 3;
+            float2 w[2][2];   // W_P^{b k}, b = 2q + h + 8 nt
+            w[0][0] = tcl_twiddle<float>(tw, (uint64_t)((uint32_t)(2 * q) * k), logP);
+            const float2 s1 = tcl_twiddle<float>(tw, (uint64_t)k, logP);
+            const float2 s8 = tcl_twiddle<float>(tw, (uint64_t)(8u * k), logP);
+            w[0][1] = cmul(w[0][0], s1);
+            w[1][0] = cmul(w[0][0], s8);
+            w[1][1] = cmul(w[1][0], s1);
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) t[nt][i] = cmul(t[nt][i], w[nt][i & 1]);
+        }
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const float2 u = cmul(mkc(s.acc[0][nt][i], s.acc[1][nt][i]), c.itw[nt][i]);
+                const float2 u = cmul(mkc(s.acc[0][nt][i], s.acc[1][nt][i]), t[nt][i]);
                 s.acc[0][nt][i] = u.x;
                 s.acc[1][nt][i] = u.y;
             }
@@ -286,15 +421,29 @@ struct TcLean {
     }
 
     // Phase 4: unscale (with the pass's output factor and conjugation) into
-    // the line's shared slots, in place.
+    // the line's shared slots, in place.  slot = base + (lx ^ ((i & 1) | nt << 3))
+    // + (((i & 1) + 8 nt + 128 (i >> 1)) << 4).
     static NFFT_HD void store(const PassArgs& a, float2* sm, int l, int lane, const LineRegs& s) {
-        const float f = ldexpf((float)a.scale, -s.e);
+        const int g = lane >> 2, q = lane & 3;
+        float2* base = sm + ((2 * q + 16 * g) << 4);
+        const int lx = l ^ (g & 1) ^ (q << 1) ^ (((g >> 1) & 1) << 3);
+        const bool plain = s.e == 0 && a.scale == 1.0 && !a.conj_out;
+        const float f = (float)a.scale * tcl_pow2(-s.e);
         const float fi = a.conj_out ? -f : f;
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-                sm[NFFT_SM(tcl_slot(out_point(lane, nt, i), l))] = mkc(s.acc[0][nt][i] * f, s.acc[1][nt][i] * fi);
+            for (int c = 0; c < 2; ++c) {
+                float2* p = base + (lx ^ (c | (nt << 3)));
+#pragma unroll
+                for (int hi = 0; hi < 2; ++hi) {
+                    const int i = c + 2 * hi;
+                    const int off = (c + 8 * nt + 128 * hi) << 4;
+                    const float2 v = plain ? mkc(s.acc[0][nt][i], s.acc[1][nt][i])
+                                           : mkc(s.acc[0][nt][i] * f, s.acc[1][nt][i] * fi);
+                    tcl_at(sm, p, off) = v;
+                }
+            }
     }
 
 #if defined(__CUDA_ARCH__)
@@ -307,69 +456,173 @@ struct TcLean {
         for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
         split1(m, s);
         tcl_stage(c.A, s.xb, s.acc);
-        mid(c, s);
+        mid(a, tw, c, j, lane, s);
         tcl_stage(c.A, s.xb, s.acc);
         store(a, sm, l, lane, s);
     }
 #endif
 };
 
-// One tile (16 lines) of a radix-256 split tensor-core pass.  The input is
-// read once (coalesced: lines fastest in column mode, points fastest in row
-// mode), every warp transforms its lines in shared memory, and the tile is
-// written once with the matching mapping of the output side.
+
+// Store with an L2 policy (one instruction; the policy encodes the pass's
+// hint: evict_first for user data, evict_last for kept scratch).
+__device__ __forceinline__ void tcl_st(float2* p, float2 v, uint64_t pol) {
+#if defined(__CUDA_ARCH__)
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol)
+                 : "memory");
+#endif
+}
+
+// Two adjacent points in one 16-byte store (p 16-byte aligned).
+__device__ __forceinline__ void tcl_st2(float2* p, float2 v0, float2 v1, uint64_t pol) {
+#if defined(__CUDA_ARCH__)
+    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(v0.x), "f"(v0.y), "f"(v1.x),
+                 "f"(v1.y), "l"(pol)
+                 : "memory");
+#endif
+}
+
+// 8-byte asynchronous copy global -> shared (shared-window address dst).
+__device__ __forceinline__ void tcl_cp8s(uint32_t dst, const float2* src, uint64_t pol) {
+#if defined(__CUDA_ARCH__)
+    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "l"(pol)
+                 : "memory");
+#endif
+}
+
+// The pipeline of a persistent CTA over 16-line tiles, with two shared
+// buffers: the copies of tile k+1 are in flight while tile k is transformed
+// and written out.
+//  lines()    the first 16 threads resolve a tile's lines once: offset of
+//             point 0 on each side, or -1 past the last line, and j;
+//  prefetch() every thread issues its 16 asynchronous copies.  Column mode
+//             (16 adjacent lines make 128-byte rows): thread t copies line
+//             t & 15, points (t >> 4) + 16 it.  Row mode (each line one run):
+//             thread t copies point t of every line.  Slot (r0 + 16 it, l)
+//             sits at (r0 << 4) + (it << 8) + ((l ^ S(r0)) ^ c_it), c_it =
+//             (it & 1) | (it & 2) << 2: one XOR per element against a
+//             per-thread constant;
+//  compute()  every warp transforms its lines in place;
+//  writeout() the tile written once with the matching walk of the output side.
 template <int THREADS>
-__device__ __forceinline__ void tc_lean_tile(const PassArgs& a, const typename TcLean<THREADS>::Consts& c,
-                                             long long tile, float2* sm, long long* lin) {
+struct TcPipe {
     using TL = TcLean<THREADS>;
-    const TwTables<float>* tw = (const TwTables<float>*)a.tw;
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    long long* lout = lin + TCL_J;
-    long long* lj = lout + TCL_J;
-    if (t < TCL_J) line_setup(a, (tile << TCL_LOGJ) + t, t, TileLines{lin, lout, lj});
-    __syncthreads();
-    // load: a batch of loads in flight before its shared stores
-    {
-        constexpr int BATCH = TL::PER_THREAD >= 8 ? 8 : TL::PER_THREAD;
-#pragma unroll 1
-        for (int b0 = 0; b0 < TL::PER_THREAD; b0 += BATCH) {
-            float2 buf[BATCH];
-#pragma unroll
-            for (int it = 0; it < BATCH; ++it) {
-                int l, r;
-                tcl_walk(a.in_row, t + (b0 + it) * THREADS, l, r);
-                const long long j = lj[l];
-                if (j < 0) {
-                    buf[it] = mkc(0.0f, 0.0f);
-                } else {
-                    buf[it] = gload((const float2*)a.in + tcl_in_off(a, lin[l], j, r), a.hint_in);
-                    if (a.conj_in) buf[it].y = -buf[it].y;
-                }
+    static_assert(THREADS == TCL_R, "one thread per point of a line in the row walks");
+
+    static __device__ __forceinline__ void lines(const PassArgs& a, long long tile, long long* lb) {
+        const int t = threadIdx.x;
+        if (t < TCL_J) {
+            long long bin, bout, j;
+            const long long lam = (tile << TCL_LOGJ) + t;
+            if (a.ndims == 2 && a.jpos == 0 && a.cnt[0] == (1ll << a.logNj) && !a.in_tab && !a.out_tab) {
+                // j innermost over the 2^logNj lines of a transform, one batch
+                // dimension: shifts instead of the generic divisions
+                const long long bt = lam >> a.logNj;
+                j = lam < a.nlines ? (lam & (a.cnt[0] - 1)) : -1;
+                bin = bt * a.istr[1];
+                bout = bt * a.ostr[1];
+            } else {
+                line_setup(a, lam, 0, TileLines{&bin, &bout, &j});
             }
+            const int logNso = a.logNs_out;
+            const long long base = ((j >> logNso) << (logNso + TCL_LOGR)) + (j & ((1ll << logNso) - 1));
+            lb[t] = j < 0 ? -1 : bin + j * a.in_estride;
+            lb[TCL_J + t] = j < 0 ? -1 : bout + base * a.out_estride;
+            lb[2 * TCL_J + t] = j;
+        }
+    }
+
+    static __device__ __forceinline__ void prefetch(const PassArgs& a, const long long* lb, float2* buf, uint64_t pol) {
+        const int t = threadIdx.x;
+        const float2* in = (const float2*)a.in;
+        const long long irs = a.in_estride << a.logNj;
+        if (!a.in_row) {
+            const int l = t & (TCL_J - 1), r0 = t >> TCL_LOGJ;
+            const long long b = lb[l];
+            const int sx = l ^ tcl_swz(r0);
+            float2* sp = buf + (r0 << TCL_LOGJ);
+            if (b < 0) {
 #pragma unroll
-            for (int it = 0; it < BATCH; ++it) {
-                int l, r;
-                tcl_walk(a.in_row, t + (b0 + it) * THREADS, l, r);
-                sm[NFFT_SM(tcl_slot(r, l))] = buf[it];
+                for (int k = 0; k < TCL_J; ++k) sp[(k << 8) + (sx ^ ((k & 1) | ((k & 2) << 2)))] = mkc(0.0f, 0.0f);
+                return;
+            }
+            // four shared bases (sx ^ c, c in {0, 1, 8, 9}) plus immediates
+            const uint32_t s0 = (uint32_t)__cvta_generic_to_shared(sp);
+            const uint32_t sa[4] = {s0 + ((uint32_t)(sx ^ 0) << 3), s0 + ((uint32_t)(sx ^ 1) << 3),
+                                    s0 + ((uint32_t)(sx ^ 8) << 3), s0 + ((uint32_t)(sx ^ 9) << 3)};
+            const float2* gp = in + b + r0 * irs;
+            const long long st = (long long)TCL_J * irs;
+#pragma unroll
+            for (int k = 0; k < TCL_J; ++k) {
+                tcl_cp8s(sa[(k & 1) | (k & 2)] + ((uint32_t)k << 11), gp, pol);
+                gp += st;
+            }
+        } else {
+            const int r = t, sr = tcl_swz(r);
+            float2* sp = buf + (r << TCL_LOGJ);
+            const uint32_t s0 = (uint32_t)__cvta_generic_to_shared(sp);
+            const long long roff = r * irs;
+#pragma unroll
+            for (int k = 0; k < TCL_J; ++k) {
+                const long long b = lb[k];
+                if (b < 0) sp[k ^ sr] = mkc(0.0f, 0.0f);
+                else tcl_cp8s(s0 + ((uint32_t)(k ^ sr) << 3), in + b + roff, pol);
             }
         }
     }
-    __syncthreads();
+
+    static __device__ __forceinline__ void compute(const PassArgs& a, const typename TL::Consts& c, const long long* lb,
+                                                   float2* buf) {   // c: this lane's constants (shared)
+        const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+        const TwTables<float>* tw = (const TwTables<float>*)a.tw;
 #pragma unroll 1
-    for (int k = 0; k < TL::LPW; ++k) {
-        const int l = warp + k * TL::WARPS;
-        if (lj[l] >= 0) TL::line(a, tw, c, sm, l, lj[l], lane);
+        for (int k = 0; k < TL::LPW; ++k) {
+            const int l = warp + k * TL::WARPS;
+            const long long j = lb[2 * TCL_J + l];
+            if (j >= 0) TL::line(a, tw, c, buf, l, j, lane);
+        }
     }
-    __syncthreads();
-    // store
-#pragma unroll 4
-    for (int it = 0; it < TL::PER_THREAD; ++it) {
-        int l, r;
-        tcl_walk(a.out_row, t + it * THREADS, l, r);
-        const long long j = lj[l];
-        if (j < 0) continue;
-        gstore((float2*)a.out + tcl_out_off(a, lout[l], j, r), sm[NFFT_SM(tcl_slot(r, l))], a.hint_out);
+
+    static __device__ __forceinline__ void writeout(const PassArgs& a, const long long* lb, const float2* buf,
+                                                    uint64_t pol) {
+        const int t = threadIdx.x;
+        float2* out = (float2*)a.out;
+        const long long ors = a.out_estride << a.logNs_out;
+        if (!a.out_row) {
+            const int l = t & (TCL_J - 1), r0 = t >> TCL_LOGJ;
+            const long long b = lb[TCL_J + l];
+            if (b < 0) return;
+            const int sx = l ^ tcl_swz(r0);
+            const float2* sp = buf + (r0 << TCL_LOGJ);
+            const float2* sc[4] = {sp + (sx ^ 0), sp + (sx ^ 1), sp + (sx ^ 8), sp + (sx ^ 9)};
+            float2* gp = out + b + r0 * ors;
+            const long long st = (long long)TCL_J * ors;
+#pragma unroll
+            for (int k = 0; k < TCL_J; ++k) {
+                tcl_st(gp, sc[(k & 1) | (k & 2)][k << 8], pol);
+                gp += st;
+            }
+        } else {
+            // point pairs (2p, 2p + 1) of lines l = (t >> 7) + 2 it: 16-byte
+            // stores when the line starts on a pair boundary.  S(2p + 1) = S(2p) ^ 1.
+            const int pp = t & 127, r = 2 * pp, s2 = tcl_swz(r);
+            const float2* sp0 = buf + (r << TCL_LOGJ);
+            const float2* sp1 = sp0 + TCL_J;
+#pragma unroll
+            for (int it = 0; it < TCL_J / 2; ++it) {
+                const int l = (t >> 7) + 2 * it;
+                const long long b = lb[TCL_J + l];
+                if (b < 0) continue;
+                const float2 v0 = sp0[l ^ s2], v1 = sp1[l ^ s2 ^ 1];
+                float2* gp = out + b + r * ors;
+                if (ors == 1 && (((uintptr_t)gp) & 15) == 0) tcl_st2(gp, v0, v1, pol);
+                else {
+                    tcl_st(gp, v0, pol);
+                    tcl_st(gp + ors, v1, pol);
+                }
+            }
+        }
     }
-}
+};
 
 }  // namespace nfft

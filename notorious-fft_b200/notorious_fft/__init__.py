@@ -43,7 +43,8 @@ EXTENSION_SYMBOLS = (
        "notorious_fft_dft_noalloc", "notorious_fft_mkbatch", "notorious_fft_batch_in_size",
        "notorious_fft_batch_out_size", "notorious_fft_batch_execute", "notorious_fft_batch_status",
        "notorious_fft_batch_set_graph", "notorious_fft_batch_info", "notorious_fft_free_batch",
-       "notorious_fft_batch_debug_withhold", "notorious_fft_autotune", "notorious_fft_tune_lookup"]
+       "notorious_fft_batch_debug_withhold", "notorious_fft_autotune", "notorious_fft_tune_lookup",
+       "notorious_fft_tune_lookup_plan", "notorious_fft_aux_schedule"]
 )
 
 
@@ -110,6 +111,11 @@ class Library:
         L.notorious_fft_batch_debug_withhold.restype = I
         L.notorious_fft_autotune.argtypes, L.notorious_fft_autotune.restype = [I, I], I
         L.notorious_fft_tune_lookup.argtypes, L.notorious_fft_tune_lookup.restype = [I, I, ctypes.POINTER(I), I], I
+        PI = ctypes.POINTER(I)
+        L.notorious_fft_tune_lookup_plan.argtypes = [I, I, PI, I, PI]
+        L.notorious_fft_tune_lookup_plan.restype = I
+        L.notorious_fft_aux_schedule.argtypes = [V, I, PI, I, PI]
+        L.notorious_fft_aux_schedule.restype = I
         self.real_size = L.notorious_fft_real_size()
         self.single = self.real_size == 4
         self.rdt = np.float32 if self.single else np.float64
@@ -153,6 +159,15 @@ class Library:
         buf = (ctypes.c_int * 4)()
         k = self.lib.notorious_fft_tune_lookup(KIND_CODE[kind], int(n), buf, 4)
         return [buf[i] for i in range(min(k, 4))]
+
+    def tune_lookup_plan(self, kind: str, n: int):
+        """(split, logt) cached for standalone plans of kind's family and n, or None."""
+        buf = (ctypes.c_int * 4)()
+        lt = ctypes.c_int(0)
+        k = self.lib.notorious_fft_tune_lookup_plan(KIND_CODE[kind], int(n), buf, 4, ctypes.byref(lt))
+        if k < 0:
+            return None
+        return [buf[i] for i in range(min(k, 4))], lt.value
 
     def mkaux_raw(self, fam: str, dims: Sequence[int]):
         """The raw pointer (or None) -- mirrors the C convention of returning NULL."""
@@ -230,6 +245,15 @@ class Aux:
     @property
     def form(self) -> int:
         return self.L.lib.notorious_fft_get_form(self.ptr)
+
+    def schedule(self, axis: int = -1):
+        """(pass radices log2, threads log2 or 0) of an axis's inner power-of-two FFT."""
+        buf = (ctypes.c_int * 4)()
+        lt = ctypes.c_int(0)
+        k = self.L.lib.notorious_fft_aux_schedule(self.ptr, int(axis), buf, 4, ctypes.byref(lt))
+        if k < 0:
+            self.L.check()
+        return [buf[i] for i in range(min(k, 4))], lt.value
 
     # shapes of one transform
     def in_shape(self, kind: str) -> tuple:

@@ -851,10 +851,7 @@ bool launch_tc_lean(const PassArgs& a, int, cudaStream_t) {
                 int l, r;
                 tcl_walk(a.in_row, e, l, r);
                 float2 v = make_float2(0.f, 0.f);
-                if (lj[l] >= 0) {
-                    v = NFFT_GLD((const float2*)a.in + tcl_in_off(a, lin[l], lj[l], r));
-                    if (a.conj_in) v.y = -v.y;
-                }
+                if (lj[l] >= 0) v = NFFT_GLD((const float2*)a.in + tcl_in_off(a, lin[l], lj[l], r));
                 sm[NFFT_SM(tcl_slot(r, l))] = v;
             }
             for (int l = 0; l < TCL_J; ++l) {
@@ -868,7 +865,7 @@ bool launch_tc_lean(const PassArgs& a, int, cudaStream_t) {
                 emu_tcl_stage(A, xb, acc);
                 for (int lane = 0; lane < 32; ++lane) {
                     memcpy(st[lane].acc, acc[lane], sizeof acc[lane]);
-                    TL::mid(c[lane], st[lane]);
+                    TL::mid(a, tw, c[lane], lj[l], lane, st[lane]);
                     memcpy(xb[lane], st[lane].xb, sizeof xb[lane]);
                 }
                 emu_tcl_stage(A, xb, acc);
