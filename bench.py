@@ -1,7 +1,7 @@
 """Benchmark of the B200 FFT engine (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2c|c1]
+                    [--workload c2c|c1|ragged|split_tc]
 
 Workloads (synthetic, seeded; no dataset is involved):
   c2c  (default) batched complex DFT, FP64, N = 65536 x 4096 transforms per
@@ -46,6 +46,8 @@ WORKLOADS = {
     "c1": dict(N=4096, batch=256, l2="L2 flushed (256 MiB write) between steps", flush=True),
     # ragged batch in one persistent launch; `batch` = number of transforms
     "ragged": dict(N=0, batch=20000, l2="L2 flushed (256 MiB write) between steps", flush=True),
+    # profiling workload: the float library's precision forms on N = 65536 x batch
+    "split_tc": dict(N=65536, batch=512, l2="inputs 256 MiB per array > L2 (no flush)", flush=False),
 }
 
 
@@ -600,6 +602,38 @@ def run_ragged(args, wl):
     b.free()
 
 
+def run_split_tc(args, wl):
+    """Profiling workload: the float library's split tensor-core form (or, with
+    --form plain, the plain FP32 form) on a batch of N = 65536 complex
+    transforms, dft only; prints the time per call."""
+    import torch
+
+    from notorious_fft import FORM_SPLIT_TC, load
+
+    L = load(single=True)
+    stream = torch.cuda.current_stream()
+    L.set_stream(stream.cuda_stream)
+    N, B = wl["N"], wl["batch"]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    x = torch.randn(B, N, generator=g, device="cuda", dtype=torch.complex64)
+    y = torch.empty_like(x)
+    with L.mkaux("dft", [N]) as a:
+        a.set_form(0 if args.form == "plain" else FORM_SPLIT_TC)
+        for _ in range(args.warmup):
+            a.batched("dft", x, y, B, N, N)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            a.batched("dft", x, y, B, N, N)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"workload": f"{args.form} fp32 N={N} x{B} dft", "ms": round(ms, 4),
+                      "gb_s": round(B * N * 16 / (ms * 1e-3) / 1e9, 1)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -608,6 +642,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2c")
     ap.add_argument("--batch", type=int, default=0, help="override the workload's batch (profiling runs)")
+    ap.add_argument("--form", choices=["split_tc", "plain"], default="split_tc",
+                    help="precision form of the split_tc profiling workload")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the float-library forms")
@@ -622,6 +658,8 @@ def main():
         return run_reference_arm(args, wl)
     if args.workload == "ragged":
         return run_ragged(args, wl)
+    if args.workload == "split_tc":
+        return run_split_tc(args, wl)
 
     import numpy as np
     import torch

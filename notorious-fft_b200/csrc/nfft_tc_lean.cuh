@@ -65,7 +65,7 @@ NFFT_HD int tcl_slot(int r, int l) {
 
 // Two tile buffers, two sets of line offsets, and the per-lane constants
 // (F fragments and internal twiddles, 32 lanes; see TcLean::Consts).
-constexpr size_t TCL_CONSTS_BYTES = 32 * 256;
+constexpr size_t TCL_CONSTS_BYTES = 32 * 176;
 template <int THREADS>
 constexpr size_t tcl_smem_bytes() {
     return 2 * (sizeof(float2) * (size_t)TCL_SLOTS + sizeof(long long) * 3 * (size_t)TCL_J) + TCL_CONSTS_BYTES;
@@ -97,7 +97,7 @@ NFFT_HD void tcl_split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
 
 NFFT_HD void tcl_mma(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
 #if defined(__CUDA_ARCH__)
-    asm volatile(
+    asm(
         "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
         "{%0, %1, %2, %3};"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
@@ -109,7 +109,7 @@ NFFT_HD void tcl_mma(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
 // d = a b (zero accumulator)
 NFFT_HD void tcl_mma0(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
 #if defined(__CUDA_ARCH__)
-    asm volatile(
+    asm(
         "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
         "{%10, %10, %10, %10};"
         : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
@@ -240,6 +240,8 @@ struct TcLean {
     struct __align__(16) Consts {
         TcA A;
         float2 itw[2][4];
+        uint32_t pad[4];   // 176-byte stride (11 x 16): the lanes' 16-byte reads of a
+                           // quarter warp fall on 8 distinct bank groups
     };
     static_assert(32 * sizeof(Consts) <= TCL_CONSTS_BYTES, "constants table");
 
