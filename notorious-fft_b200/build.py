@@ -27,9 +27,8 @@ BUILD = os.path.join(HERE, "_build")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 QUEUE_BRANCHES = [f"nfft_queue_b{k}.cu" for k in range(5)]
-SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu", "nfft_noalloc.cu", "nfft_cluster.cu", "nfft_tc.cu",
-           "nfft_queue_build.cu", "nfft_queue_kernel.cu", "nfft_resident.cu", "nfft_resident_a.cu",
-           "nfft_resident_b.cu", "nfft_resident_t.cu", "nfft_mid.cu"] + QUEUE_BRANCHES + [f"nfft_lean_s{k}.cu" for k in range(8)]
+SOURCES = ["nfft_kernels.cu", "nfft_plan.cu", "nfft_api.cu", "nfft_noalloc.cu", "nfft_tc.cu",
+           "nfft_queue_build.cu", "nfft_queue_kernel.cu"] + QUEUE_BRANCHES + [f"nfft_lean_s{k}.cu" for k in range(8)]
 # The persistent queue kernel and its branch functions are relocatable device
 # code (linked by nvcc -dlink), so the branch units compile in parallel.  They
 # read data that other CTAs wrote earlier in the same launch: global loads

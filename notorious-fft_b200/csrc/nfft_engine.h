@@ -130,9 +130,6 @@ struct notorious_fft_plan {
     // temporary of the multi-dimensional inverse real transform
     void* nd_tmp = nullptr;
     size_t nd_tmp_bytes = 0;
-    // counters of the resident two-pass kernel
-    unsigned* res_ctr = nullptr;
-    size_t res_ctr_n = 0;
     // ordering across streams: the scratch above is shared by every call on
     // this plan, so a call on another stream than the previous call's first
     // waits for the event recorded at the end of that call
@@ -222,28 +219,6 @@ struct QueueArgs;
 int queue_grid(const DeviceCtx* c);   // resident CTAs (0 on error)
 bool launch_queue(const QueueArgs& q, int grid, cudaStream_t s);
 
-// Resident two-pass kernels (nfft_resident.cu): both Stockham passes of a
-// batched power-of-two complex DFT in one persistent launch, the inter-pass
-// scratch kept in L2.  ctr: B + 3 counters of device memory.
-struct ResidentEntry {
-    int r1, r2, logt;
-    const void* fn;         // plain resident kernel
-    size_t smem;
-    const void* fn_pf;      // software-pipelined variant (cp.async staging)
-    size_t smem_pf;
-};
-const ResidentEntry* resident_find(int r1, int r2);
-// Resident kernels fed by tensor copies: NG consumer groups, S stage buffers.
-struct ResidentTmaEntry {
-    int r1, r2, logt, ng, stages;
-    const void* fn;
-    size_t smem;
-};
-const ResidentTmaEntry* resident_tma_find(int r1, int r2);
-bool resident_set_attributes();
-bool launch_resident(const DeviceCtx* c, const PassArgs& a1, const PassArgs& a2, int r1, int r2, long long B,
-                     unsigned* ctr, cudaStream_t s);
-
 // Ragged batches (nfft_queue_build.cu).  Offsets in reals, NULL: packed.
 notorious_fft_batch* batch_create_default(int count, const int* kinds, const int* Ns, const long long* in_off,
                                           const long long* out_off);
@@ -273,17 +248,12 @@ PlanOverride*& plan_override();
 long long launch_count();
 void note_launch();
 
-// Cluster-resident complex DFT (nfft_cluster.cu): one transform of 2^logN
-// points per thread-block cluster; a1 / a2 are its two Stockham passes.
-bool cluster_available(int logN);
 // Split-tensor-core pass (nfft_tc.cu, float library): LD_C / ST_C passes.
 bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStream_t s);
 // Radix-256 passes of the split tensor-core form (16-line tiles, persistent
 // CTAs, nfft_tc_lean.cuh); NOTORIOUS_FFT_TC_LEAN=0 selects tc_pass_kernel.
 bool tc_lean_enabled();
 bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s);
-int cluster_logr1(int logN);
-bool launch_cluster(const PassArgs& a1, const PassArgs& a2, int logN, long long ntransforms, cudaStream_t s);
 
 // Specialized pass kernels (nfft_lean.cuh), registered by the slice files.
 constexpr int NFFT_LEAN_SLICES = 8;
@@ -309,11 +279,6 @@ const LeanRegistry& lean_registry();
 // Launch the specialized kernel for this pass shape, or return false with no
 // error set when none is instantiated (the caller then uses pass_kernel).
 bool lean_available(int logR, int logT, int ci, int co, int ld, int st);
-// Bluestein middle kernels (nfft_mid.cu): forward last pass + filter product +
-// first pass of the second FFT in one launch (a1 / a2: the two passes).
-bool lean_mid_available(int logR);
-bool mid_set_attributes();
-bool launch_lean_mid(PassArgs a1, PassArgs a2, int logR, cudaStream_t s);
 bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, long long ntiles, cudaStream_t s);
 
 }  // namespace nfft

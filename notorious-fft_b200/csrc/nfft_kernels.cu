@@ -101,7 +101,6 @@ bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, lo
 }
 
 bool set_kernel_attributes() {
-    if (!resident_set_attributes() || !mid_set_attributes()) return false;
     for (auto& kv : lean_registry().entries) {
         if (!cuda_ok(cudaFuncSetAttribute(kv.second.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kv.second.smem),
                      "cudaFuncSetAttribute(lean pass)"))

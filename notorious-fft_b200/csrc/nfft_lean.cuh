@@ -574,164 +574,6 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
     }
 }
 
-// Bluestein middle of a multi-pass convolution in one tile: the last pass of
-// the forward M-point FFT (radix R, Ns = M/R, column tiles), the filter product
-// and conjugation, and the first pass of the second FFT (radix R, Ns = 1).
-// The forward pass writes Y[j + r M/R] of its J lines to shared memory in
-// natural order, which is exactly what the second FFT's first pass reads for
-// the same lines, so the product never leaves the tile (one sweep of M fewer
-// than two separate passes).  a1: forward pass (input = scratch), a2: second
-// pass (output = scratch, row layout); both over the same lines.
-template <typename T, int LOGR, int LOGT>
-struct LeanMid {
-    using L1 = Lean<T, LOGR, LOGT, true, true, LD_C, ST_C>;
-    using L2 = Lean<T, LOGR, LOGT, true, false, LD_C, ST_C>;
-    static_assert(L1::NS >= 2 && L1::SMEM_ELEMS == L2::SMEM_ELEMS, "middle tile shapes");
-    static constexpr int J = L1::J, LOGJ = L1::LOGJ, THREADS = L1::THREADS;
-    static constexpr size_t SMEM_BYTES = sizeof(C2<T>) * (size_t)L1::SMEM_ELEMS + sizeof(LeanLine) * (size_t)J;
-    // slot e of the filter phase -> (line, r): lines fastest
-    static NFFT_HD void slot(int e, int& l, int& r) {
-        l = e & (J - 1);
-        r = e >> LOGJ;
-    }
-    static NFFT_HD void filter(const PassArgs& a1, C2<T>* sm, const LeanLine* lines, int e) {
-        int l, r;
-        slot(e, l, r);
-        const LeanLine ln = lines[l];
-        if (ln.j < 0) return;
-        const long long p = ln.j + ((long long)r << a1.logNj);
-        C2<T>& x = sm[NFFT_SM((lean_idx<true, LOGR, LOGJ>(l, r)))];
-        x = cconj(cmul(x, gload_keep(&((const C2<T>*)a1.filt)[p])));
-    }
-};
-
-#if defined(__CUDACC__)
-template <typename T, int LOGR, int LOGT>
-__device__ __forceinline__ void lean_mid_tile(const PassArgs& a1, const PassArgs& a2, long long tile,
-                                              unsigned char* smraw) {
-    using M = LeanMid<T, LOGR, LOGT>;
-    using L1 = typename M::L1;
-    using L2 = typename M::L2;
-    using V = C2<T>;
-    V* sm = (V*)smraw;
-    LeanLine* lines = (LeanLine*)(sm + L1::SMEM_ELEMS);
-    const TwTables<T>* tw = (const TwTables<T>*)a1.tw;
-    const int t = threadIdx.x;
-    const long long line0 = tile << M::LOGJ;
-    if (line0 >= a1.nlines) return;
-    if (t < M::J) {
-        long long t1[3], t2[3];
-        line_setup(a1, line0 + t, 0, TileLines{&t1[0], &t1[1], &t1[2]});
-        line_setup(a2, line0 + t, 0, TileLines{&t2[0], &t2[1], &t2[2]});
-        lines[t] = LeanLine{t1[0], t2[1], t1[2]};
-    }
-    __syncthreads();
-    V v[16];
-    int l, i;
-    // forward FFT, last pass: outputs to shared memory in natural order
-    L1::first(a1, tw, lines, t, v, l, i);
-    L1::template write_smem<0>(sm, l, i, v);
-    __syncthreads();
-    if constexpr (L1::NS >= 3) {
-        constexpr int S = 1;
-        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-        V w[16];
-        int ls[16 / RHO], is[16 / RHO];
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) L1::template read<S, true>(sm, t, q, &w[q * RHO], ls[q], is[q]);
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) {
-            L1::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
-            L1::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
-        }
-        __syncthreads();
-    }
-    if constexpr (L1::NS >= 4) {
-        constexpr int S = 2;
-        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-        V w[16];
-        int ls[16 / RHO], is[16 / RHO];
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) L1::template read<S, true>(sm, t, q, &w[q * RHO], ls[q], is[q]);
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) {
-            L1::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
-            L1::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
-        }
-        __syncthreads();
-    }
-    {
-        constexpr int S = L1::NS - 1;
-        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-        V w[16];
-        int ls[16 / RHO], is[16 / RHO];
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) L1::template read<S, true>(sm, t, q, &w[q * RHO], ls[q], is[q]);
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) {
-            L1::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
-            L1::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
-        }
-    }
-    __syncthreads();
-    // filter product and conjugation in place
-    for (int e = t; e < (M::J << LOGR); e += M::THREADS) M::filter(a1, sm, lines, e);
-    __syncthreads();
-    // second FFT, first pass (no pre-twiddle): radix 16 from shared memory
-    L2::template read<0, true>(sm, t, 0, v, l, i);
-    __syncthreads();
-    L2::pre_twiddle_dft(a2, tw, 0, i, v);
-    L2::template write_smem<0>(sm, l, i, v);
-    __syncthreads();
-    if constexpr (L2::NS >= 3) {
-        constexpr int S = 1;
-        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-        V w[16];
-        int ls[16 / RHO], is[16 / RHO];
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) L2::template read<S, true>(sm, t, q, &w[q * RHO], ls[q], is[q]);
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) {
-            L2::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
-            L2::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
-        }
-        __syncthreads();
-    }
-    if constexpr (L2::NS >= 4) {
-        constexpr int S = 2;
-        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-        V w[16];
-        int ls[16 / RHO], is[16 / RHO];
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) L2::template read<S, true>(sm, t, q, &w[q * RHO], ls[q], is[q]);
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) {
-            L2::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
-            L2::template write_smem<S>(sm, ls[q], is[q], &w[q * RHO]);
-        }
-        __syncthreads();
-    }
-    {
-        constexpr int S = L2::NS - 1;
-        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-        V w[16];
-        int ls[16 / RHO], is[16 / RHO];
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) L2::template read<S, false>(sm, t, q, &w[q * RHO], ls[q], is[q]);
-#pragma unroll
-        for (int q = 0; q < 16 / RHO; ++q) {
-            L2::template twiddle_dft<S>(tw, is[q], &w[q * RHO]);
-            L2::template write_global<S>(a2, tw, lines, ls[q], is[q], &w[q * RHO]);
-        }
-    }
-}
-#endif
-
 // Minimum CTAs per SM the specialized kernels are compiled for (register
 // budget 65536 / (threads x CTAs)).  The passes are latency-bound, so warps per
 // SM matter: the float kernels fit in 64 registers and run 8 CTAs of 128
@@ -765,13 +607,6 @@ lean_pass_kernel(const PassArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     lean_tile<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>(a, (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x,
                                                            smraw);
-}
-
-template <typename T, int LOGR, int LOGT>
-__global__ void __launch_bounds__(1 << LOGT, (lean_min_blocks<T, LOGT>()))
-lean_mid_kernel(const PassArgs a1, const PassArgs a2) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    lean_mid_tile<T, LOGR, LOGT>(a1, a2, (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x, smraw);
 }
 
 }  // namespace nfft

@@ -304,21 +304,6 @@ static void set_lines(PassArgs& a, const View& src, const View& dst, long long n
     a.nlines = n;
 }
 
-// Two-pass complex transforms: one resident launch per chunk (both passes,
-// scratch in L2) when NOTORIOUS_FFT_RESIDENT=1, else two launches.  The
-// resident form halves the DRAM traffic but is bound by the SMs' tile
-// throughput, which the two launches already nearly saturate at ~90% of HBM
-// bandwidth; on B200 it is not faster than the default schedules at any size.
-static bool resident_enabled(int logL) {
-    static int v = -2;
-    if (v == -2) {
-        const char* e = getenv("NOTORIOUS_FFT_RESIDENT");
-        v = e ? (atoi(e) != 0 ? 1 : 0) : 0;
-    }
-    (void)logL;
-    return v == 1;
-}
-
 // L2 policy of multi-pass transforms: every pass that touches scratch
 // streams its user data (evict first) and keeps its scratch (evict_last
 // stores, discard after the last read).  NOTORIOUS_FFT_CACHE_HINTS: 0 never;
@@ -521,32 +506,6 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
     const FftSchedule& sch = strided ? ax.fft_strided : ax.fft_contig;
     const long long L = 1ll << logL;
     const int np = sch.npass;
-    // One transform per thread-block cluster: no inter-pass scratch at all.
-    if (np > 1 && !strided && !op.tc && op.ld == LD_C && op.st == ST_C && src.nb <= 1 && dst.nb <= 1 &&
-        !recorder() && cluster_available(logL)) {
-        const int lr1 = cluster_logr1(logL), lr2 = logL - lr1;
-        PassArgs a1, a2;
-        fill_common(a1, c);
-        fill_common(a2, c);
-        a1.in = src.ptr;
-        a1.logR = lr1;
-        a1.logNj = lr2;
-        a1.in_estride = 1;
-        a1.conj_in = op.conj_in;
-        a1.istr[0] = src.nb ? src.str[0] : 0;
-        a1.hint_in = cache_hints() ? 1 : 0;
-        a2.out = dst.ptr;
-        a2.logR = lr2;
-        a2.logNs = lr1;
-        a2.logNs_out = lr1;
-        a2.logNj = lr1;
-        a2.out_estride = 1;
-        a2.conj_out = op.conj_out;
-        a2.scale = op.scale;
-        a2.ostr[0] = dst.nb ? dst.str[0] : 0;
-        a2.hint_out = cache_hints() ? 1 : 0;
-        return launch_cluster(a1, a2, logL, src.nb ? src.cnt[0] : 1, s);
-    }
     if (np == 1 && !(op.paired && strided)) {
         OpSpec o1 = op;
         o1.logt = sch.logt;
@@ -572,13 +531,6 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
     }
     const bool paired_epilogue = op.paired && !mirror;
     const int nbuf = paired_epilogue ? (np >= 2 ? 2 : 1) : (np >= 3 ? 2 : 1);
-    // one resident launch per chunk for plain two-pass complex transforms of
-    // contiguous lines
-    const ResidentEntry* res = nullptr;
-    if (np == 2 && !strided && !paired_epilogue && op.ld == LD_C && op.st == ST_C && !op.tc && !recorder() &&
-        src.nb <= 1 && dst.nb <= 1 && resident_enabled(logL) && !lean_disabled())
-        res = resident_find(sch.plog[0], sch.plog[1]);
-    const bool use_resident = res != nullptr;
     void* buf[2] = {nullptr, nullptr};
     for (int i = 0; i < nbuf; ++i) {
         buf[i] = get_scratch(p, i, (size_t)chunk * per_outer);
@@ -593,35 +545,6 @@ static bool run_pow2_axis(notorious_fft_plan* p, const DeviceCtx* c, const AxisP
             vd.ptr = (char*)dst.ptr + (size_t)(o0 * dst.str[dst.nb - 1]) *
                                           ((op.st == ST_C || op.st == ST_R || op.st == ST_BLUE) ? sizeof(cplx_t) : sizeof(real_t));
             vd.cnt[dst.nb - 1] = cn;
-        }
-        if (use_resident) {
-            // both passes in one persistent launch, the scratch kept in L2
-            View sv = scratch_view(buf[0], vs, L, false);
-            PassArgs a1, a2;
-            make_pass_args(c, vs, sv, logL, 0, sch.plog[0], sch.nsub[0], sch.sub[0], op, true, false, 0, 0, nullptr,
-                           nullptr, false, true, a1);
-            make_pass_args(c, sv, vd, logL, sch.plog[0], sch.plog[1], sch.nsub[1], sch.sub[1], op, false, true, 0,
-                           sch.plog[0], nullptr, nullptr, true, false, a2);
-            const int lt = res->logt;
-            a1.logJ = lt + 4 - sch.plog[0];
-            a2.logJ = lt + 4 - sch.plog[1];
-            a1.hint_in = 1;
-            a1.hint_out = 2;
-            a2.hint_in = 3;
-            a2.discard_in = 1;
-            a2.hint_out = 1;
-            const long long B = vs.lines();
-            if (p->res_ctr_n < (size_t)(B + 3)) {
-                if (p->res_ctr) cudaFree(p->res_ctr);
-                p->res_ctr = nullptr;
-                p->res_ctr_n = 0;
-                if (!cuda_ok(cudaMalloc((void**)&p->res_ctr, sizeof(unsigned) * (size_t)(B + 3)),
-                             "cudaMalloc(resident counters)"))
-                    return false;
-                p->res_ctr_n = (size_t)(B + 3);
-            }
-            if (!launch_resident(c, a1, a2, sch.plog[0], sch.plog[1], B, p->res_ctr, s)) return false;
-            continue;
         }
         View cur = vs;
         int logNs = 0;
@@ -739,31 +662,13 @@ static bool run_bluestein_axis(notorious_fft_plan* p, const DeviceCtx* c, const 
             cur = out;
             bi ^= 1;
         }
-        // NOTORIOUS_FFT_BLUE_MID=1: the last forward pass, the filter product
-        // and the first inverse pass in one kernel (the product stays in the
-        // tile, one sweep of M fewer).  Off by default: the fused tile does
-        // two passes' arithmetic and runs at the SMs' tile rate, which the two
-        // separate passes already reach at ~90% of HBM bandwidth (B200,
-        // 1,000,003 x 4: 0.360 vs 0.349 ms).
-        const int lrm = f.plog[np - 1];
-        const char* mid_env = getenv("NOTORIOUS_FFT_BLUE_MID");
-        const bool fuse_mid = mid_env && atoi(mid_env) != 0;
-        if (fuse_mid && lrm == g.plog[0] && !recorder() && !lean_disabled() && lean_mid_available(lrm)) {
-            View out = scratch_view(buf[bi], vs, M, false);
-            OpSpec o = op;
-            o.conj_in = 0;
-            PassArgs a1, a2;
-            make_pass_args(c, cur, out, logM, logNs, lrm, f.nsub[np - 1], f.sub[np - 1], op, false, false, 0, logNs,
-                           ax.chirp, ax.filt, true, true, a1);
-            make_pass_args(c, cur, out, logM, 0, lrm, g.nsub[0], g.sub[0], o, true, false, 0, 0, ax.chirp, ax.filt,
-                           true, true, a2);
-            if (!launch_lean_mid(a1, a2, lrm, s)) return false;
-            cur = out;
-            bi ^= 1;
-        } else {
+        {
             // the last forward pass and the first inverse pass as separate
             // specialized passes; the filter product and conjugation are the
-            // inverse pass's load operator
+            // inverse pass's load operator.  (Fusing the two into one tile, the
+            // product never leaving shared memory, measured slower on B200:
+            // 1,000,003 x 4 0.360 vs 0.349 ms -- the fused tile does two passes'
+            // arithmetic at the SMs' tile rate.)
             View out = scratch_view(buf[bi], vs, M, false);
             if (!run_pass(c, cur, out, logM, logNs, f.plog[np - 1], f.tile[np - 1], f.nsub[np - 1], f.sub[np - 1], op,
                           false, false, 0, logNs, ax.chirp, ax.filt, s))
@@ -931,7 +836,6 @@ void plan_destroy(notorious_fft_plan* p) {
     if (p->s_h2d) cudaStreamDestroy(p->s_h2d);
     if (p->s_d2h) cudaStreamDestroy(p->s_d2h);
     if (p->nd_tmp) cudaFree(p->nd_tmp);
-    if (p->res_ctr) cudaFree(p->res_ctr);
     if (p->stage_out) cudaFree(p->stage_out);
     if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
     delete p;

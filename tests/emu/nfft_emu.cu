@@ -197,13 +197,9 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 #include "../../notorious-fft_b200/csrc/nfft_queue_build.cu"
 #include "../../notorious-fft_b200/csrc/nfft_lean.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_lean_list.h"
-#include "../../notorious-fft_b200/csrc/nfft_cluster.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_tc.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_tc_lean.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_queue.h"
-#include "../../notorious-fft_b200/csrc/nfft_resident.cuh"
-#include "../../notorious-fft_b200/csrc/nfft_resident_list.h"
-#include "../../notorious-fft_b200/csrc/nfft_resident_tma.cuh"
 
 // ---------------------------------------------------------------------------
 // emulated launches: the kernels' phase functions for every thread
@@ -448,191 +444,6 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
     }
 }
 
-template <typename X> struct template_type_tag { using type = X; };
-// ---- Bluestein middle kernels (lean_mid_tile of nfft_lean.cuh): the forward
-// last pass, the filter product and the second FFT's first pass, every phase
-// for all threads; the two passes' line maps must agree.
-static long long g_mid_launches = 0;
-template <int LOGR, int LOGT>
-static void emu_lean_mid(const PassArgs& a1, const PassArgs& a2) {
-    using T = real_t;
-    using V = C2<T>;
-    using Mid = LeanMid<T, LOGR, LOGT>;
-    using L1 = typename Mid::L1;
-    using L2 = typename Mid::L2;
-    const TwTables<T>* tw = (const TwTables<T>*)a1.tw;
-    constexpr int TH = Mid::THREADS;
-    g_smem_elems = L1::SMEM_ELEMS;
-    std::vector<V> sm(L1::SMEM_ELEMS);
-    std::vector<LeanLine> lines(Mid::J);
-    std::vector<V> regs((size_t)TH * 16);
-    std::vector<int> ls((size_t)TH * 16), is((size_t)TH * 16);
-    auto stage = [&](auto Lc, auto Sc, auto Cc, bool to_global, const PassArgs& a) {
-        using L = typename decltype(Lc)::type;
-        constexpr int S = decltype(Sc)::value;
-        constexpr bool COLMAP = decltype(Cc)::value;
-        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-        for (int t = 0; t < TH; ++t)
-            for (int q = 0; q < 16 / RHO; ++q)
-                L::template read<S, COLMAP>(sm.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
-        for (int t = 0; t < TH; ++t)
-            for (int q = 0; q < 16 / RHO; ++q) {
-                L::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
-                if (to_global)
-                    L::template write_global<S>(a, tw, lines.data(), ls[t * 16 + q], is[t * 16 + q],
-                                                &regs[t * 16 + q * RHO]);
-                else
-                    L::template write_smem<S>(sm.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
-            }
-    };
-    template_type_tag<L1> t1;
-    template_type_tag<L2> t2;
-    const long long ntiles = (a1.nlines + Mid::J - 1) >> Mid::LOGJ;
-    if (a1.nlines != a2.nlines || a1.logJ != Mid::LOGJ || a2.logJ != Mid::LOGJ) {
-        fprintf(stderr, "nfft_emu: Bluestein middle passes disagree on their lines\n");
-        abort();
-    }
-    g_launches++;
-    g_mid_launches++;
-    for (long long tile = 0; tile < ntiles; ++tile) {
-        for (auto& x : sm) x = mkc((T)NAN, (T)NAN);
-        for (int t = 0; t < Mid::J; ++t) {
-            long long u1[3], u2[3];
-            line_setup(a1, (tile << Mid::LOGJ) + t, 0, TileLines{&u1[0], &u1[1], &u1[2]});
-            line_setup(a2, (tile << Mid::LOGJ) + t, 0, TileLines{&u2[0], &u2[1], &u2[2]});
-            if (u1[2] != u2[2]) {
-                fprintf(stderr, "nfft_emu: Bluestein middle line %lld differs between the passes\n", (tile << Mid::LOGJ) + t);
-                abort();
-            }
-            lines[t] = LeanLine{u1[0], u2[1], u1[2]};
-        }
-        for (int t = 0; t < TH; ++t) {
-            L1::first(a1, tw, lines.data(), t, &regs[t * 16], ls[t * 16], is[t * 16]);
-            L1::template write_smem<0>(sm.data(), ls[t * 16], is[t * 16], &regs[t * 16]);
-        }
-        if constexpr (L1::NS >= 3) stage(t1, std::integral_constant<int, 1>{}, std::true_type{}, false, a1);
-        if constexpr (L1::NS >= 4) stage(t1, std::integral_constant<int, 2>{}, std::true_type{}, false, a1);
-        stage(t1, std::integral_constant<int, L1::NS - 1>{}, std::true_type{}, false, a1);
-        for (int e = 0; e < (Mid::J << LOGR); ++e) Mid::filter(a1, sm.data(), lines.data(), e);
-        for (int t = 0; t < TH; ++t) L2::template read<0, true>(sm.data(), t, 0, &regs[t * 16], ls[t * 16], is[t * 16]);
-        for (int t = 0; t < TH; ++t) {
-            L2::pre_twiddle_dft(a2, tw, 0, is[t * 16], &regs[t * 16]);
-            L2::template write_smem<0>(sm.data(), ls[t * 16], is[t * 16], &regs[t * 16]);
-        }
-        if constexpr (L2::NS >= 3) stage(t2, std::integral_constant<int, 1>{}, std::true_type{}, false, a2);
-        if constexpr (L2::NS >= 4) stage(t2, std::integral_constant<int, 2>{}, std::true_type{}, false, a2);
-        stage(t2, std::integral_constant<int, L2::NS - 1>{}, std::false_type{}, true, a2);
-    }
-}
-bool lean_mid_available(int logR) { return logR >= 5 && logR <= 10; }
-bool mid_set_attributes() { return true; }
-bool launch_lean_mid(PassArgs a1, PassArgs a2, int logR, cudaStream_t) {
-    const int logt = logR <= 8 ? 7 : 8;
-    a1.logJ = a2.logJ = logt + 4 - logR;
-    switch (logR) {
-    case 5: emu_lean_mid<5, 7>(a1, a2); return true;
-    case 6: emu_lean_mid<6, 7>(a1, a2); return true;
-    case 7: emu_lean_mid<7, 7>(a1, a2); return true;
-    case 8: emu_lean_mid<8, 7>(a1, a2); return true;
-    case 9: emu_lean_mid<9, 8>(a1, a2); return true;
-    case 10: emu_lean_mid<10, 8>(a1, a2); return true;
-    }
-    set_error(6, "no Bluestein middle kernel for radix 2^%d", logR);
-    return false;
-}
-
-// Middle and last sub-stages of a lean pass (nfft_cluster.cuh lean_tail),
-// every phase for all threads.
-template <typename P, bool TO_GLOBAL>
-static void emu_lean_tail(const PassArgs& a, const TwTables<real_t>* tw, std::vector<C2<real_t>>& sm,
-                          const LeanLine* lines) {
-    using V = C2<real_t>;
-    constexpr int TH = P::THREADS;
-    std::vector<V> regs((size_t)TH * 16);
-    std::vector<int> ls((size_t)TH * 16), is((size_t)TH * 16);
-    auto stage = [&](auto Sc, auto last) {
-        constexpr int S = decltype(Sc)::value;
-        constexpr bool LAST = decltype(last)::value;
-        constexpr int RHO = 1 << LeanSched<P::LOGR_>::lr[S];
-        for (int t = 0; t < TH; ++t)
-            for (int q = 0; q < 16 / RHO; ++q) {
-                if constexpr (LAST) P::template read<S, true>(sm.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
-                else P::template read<S, P::COLL>(sm.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
-            }
-        for (int t = 0; t < TH; ++t)
-            for (int q = 0; q < 16 / RHO; ++q) {
-                P::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
-                if constexpr (LAST && TO_GLOBAL)
-                    P::template write_global<S>(a, tw, lines, ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
-                else
-                    P::template write_smem<S>(sm.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
-            }
-    };
-    if constexpr (P::NS >= 3) stage(std::integral_constant<int, 1>{}, std::false_type{});
-    if constexpr (P::NS >= 4) stage(std::integral_constant<int, 2>{}, std::false_type{});
-    stage(std::integral_constant<int, P::NS - 1>{}, std::true_type{});
-}
-
-template <int R1, int R2, int LC, int LT>
-static void emu_cluster(const PassArgs& a1, const PassArgs& a2, long long ntransforms) {
-    using T = real_t;
-    using V = C2<T>;
-    using K = ClusterFFT<T, R1, R2, LC, LT>;
-    const TwTables<T>* tw = (const TwTables<T>*)a1.tw;
-    constexpr int C = 1 << LC, TH = 1 << LT;
-    g_smem_elems = K::SMEM_ELEMS;
-    std::vector<std::vector<V>> sm(C, std::vector<V>(K::SMEM_ELEMS));
-    std::vector<std::vector<LeanLine>> lines(C, std::vector<LeanLine>(K::MAXJ));
-    std::vector<V> regs((size_t)C * TH * 16);
-    std::vector<int> ls((size_t)C * TH), is((size_t)C * TH);
-    for (long long b = 0; b < ntransforms; ++b) {
-        for (int c = 0; c < C; ++c) {
-            for (auto& x : sm[c]) x = mkc((T)NAN, (T)NAN);
-            for (int l = 0; l < (1 << K::LOGJA); ++l) K::lines1(a1, b, c, l, lines[c].data());
-            for (int t = 0; t < TH; ++t) {
-                int l, i;
-                K::P1::first(a1, tw, lines[c].data(), t, &regs[((size_t)c * TH + t) * 16], l, i);
-                K::P1::template write_smem<0>(sm[c].data(), l, i, &regs[((size_t)c * TH + t) * 16]);
-            }
-            emu_lean_tail<typename K::P1, false>(a1, tw, sm[c], lines[c].data());
-        }
-        // cluster barrier; gather from every CTA's shared memory
-        for (int c = 0; c < C; ++c)
-            for (int t = 0; t < TH; ++t)
-                K::gather(a2, tw, c, t, [&](int rank) { return (const V*)sm[rank].data(); },
-                          &regs[((size_t)c * TH + t) * 16], ls[c * TH + t], is[c * TH + t]);
-        // cluster barrier; pass 2 finishes in each CTA
-        for (int c = 0; c < C; ++c) {
-            for (auto& x : sm[c]) x = mkc((T)NAN, (T)NAN);
-            for (int l = 0; l < (1 << K::LOGJC); ++l) K::lines2(a2, b, c, l, lines[c].data());
-            for (int t = 0; t < TH; ++t)
-                K::P2::template write_smem<0>(sm[c].data(), ls[c * TH + t], is[c * TH + t], &regs[((size_t)c * TH + t) * 16]);
-            emu_lean_tail<typename K::P2, true>(a2, tw, sm[c], lines[c].data());
-        }
-    }
-}
-
-bool cluster_available(int logN) {
-    // opt-in: on B200 the two-pass kernels measured faster (2^14: 3091 vs 2198 GB/s FP64)
-    const char* v = getenv("NOTORIOUS_FFT_CLUSTER");
-    if (!v || !atoi(v)) return false;
-    if (sizeof(real_t) == 4) return logN >= 14 && logN <= 17;
-    return logN >= 14 && logN <= 16;
-}
-int cluster_logr1(int logN) { return logN == 17 ? 8 : (logN == 14 ? 7 : (logN == 15 ? 7 : 8)); }
-static long long g_cluster_launches = 0;
-bool launch_cluster(const PassArgs& a1, const PassArgs& a2, int logN, long long ntransforms, cudaStream_t) {
-    g_launches++;
-    g_cluster_launches++;
-    switch (logN) {
-    case 14: emu_cluster<7, 7, 3, 7>(a1, a2, ntransforms); return true;
-    case 15: emu_cluster<7, 8, 3, 8>(a1, a2, ntransforms); return true;
-    case 16: emu_cluster<8, 8, 4, 8>(a1, a2, ntransforms); return true;
-    case 17: emu_cluster<8, 9, 4, 9>(a1, a2, ntransforms); return true;
-    }
-    set_error(6, "no cluster kernel for N = 2^%d", logN);
-    return false;
-}
 void note_launch() { g_launches++; }
 
 // ---- split tensor-core pass: a host model of mma.sync.m16n8k16 (f16 x f16
@@ -913,244 +724,6 @@ bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, lo
 }
 long long launch_count() { return g_launches; }
 
-// ---- resident two-pass kernels: the decoded work order run by one virtual
-// CTA (a short lag so the interleaved region of the order is exercised); a
-// pass-2 tile whose transform's pass-1 tiles are not all done aborts.
-static std::vector<ResidentEntry>& emu_resident_registry() {
-    static std::vector<ResidentEntry> v = [] {
-        std::vector<ResidentEntry> r;
-#define X(R1, R2, LT) r.push_back(ResidentEntry{R1, R2, LT, nullptr, 0, nullptr, 0});
-        NFFT_RESIDENT_A(X) NFFT_RESIDENT_B(X)
-#undef X
-        return r;
-    }();
-    return v;
-}
-const ResidentEntry* resident_find(int r1, int r2) {
-    for (auto& e : emu_resident_registry())
-        if (e.r1 == r1 && e.r2 == r2) return &e;
-    return nullptr;
-}
-bool resident_set_attributes() { return true; }
-static long long g_resident_launches = 0;
-
-// ---- resident kernels fed by tensor copies: the same work order; every tile
-// is staged the way the kernel stages it -- the tensor copy restated on the
-// CPU from the host's box geometry (tma_pass_geom / tma_tile_coords, every
-// source element bounds-checked, the inner coordinate's 16-byte rule
-// asserted) into a NaN-filled stage buffer -- and computed by the consumer
-// group's phases with the exchanges in place in that buffer.
-static std::vector<ResidentTmaEntry>& emu_resident_tma_registry() {
-    static std::vector<ResidentTmaEntry> v = [] {
-        std::vector<ResidentTmaEntry> r;
-#define X(R1, R2, LT, NG) \
-    r.push_back(ResidentTmaEntry{R1, R2, LT, NG, TmaRes<real_t, R1, R2, LT>::stages(NG), nullptr, \
-                                 TmaRes<real_t, R1, R2, LT>::smem_bytes(NG)});
-        NFFT_RESIDENT_TMA(X)
-#undef X
-        return r;
-    }();
-    return v;
-}
-const ResidentTmaEntry* resident_tma_find(int r1, int r2) {
-    for (auto& e : emu_resident_tma_registry())
-        if (e.r1 == r1 && e.r2 == r2) return &e;
-    return nullptr;
-}
-
-template <typename Lt, size_t STAGE, size_t TILE_BYTES>
-static void emu_tma_tile(const PassArgs& a, long long gt, long long B) {
-    using T = real_t;
-    using V = C2<T>;
-    const TwTables<T>* tw = (const TwTables<T>*)a.tw;
-    constexpr int TH = Lt::THREADS;
-    constexpr int LOGR = Lt::LOGR_;
-    static_assert(STAGE >= TILE_BYTES && STAGE >= sizeof(V) * (size_t)Lt::SMEM_ELEMS, "stage too small");
-    std::vector<V> st(STAGE / sizeof(V), mkc((T)NAN, (T)NAN));
-    g_smem_elems = (int)(STAGE / sizeof(V));
-    // the tensor copy
-    const long long bstride = a.ndims > 1 ? a.istr[1] : (1ll << (a.logNj + LOGR));
-    const TmaPassGeom g = tma_pass_geom(a.logNj, LOGR, Lt::LOGJ, B, bstride, sizeof(V));
-    int x, z;
-    tma_tile_coords(gt, Lt::LOGJ, a.logNj, x, z);
-    if ((size_t)g.box[0] * g.box[1] * g.nbox * sizeof(T) != TILE_BYTES || (x * sizeof(T)) % 16 ||
-        (g.box[0] * sizeof(T)) % 16 || x + g.box[0] > g.dim[0] || (unsigned long long)z >= g.dim[2] ||
-        g.stride_bytes[0] % 16 || g.stride_bytes[1] % 16 || a.in_estride != 1) {
-        fprintf(stderr, "nfft_emu: tensor copy of tile %lld breaks the box rules (x %d z %d)\n", gt, x, z);
-        abort();
-    }
-    T* sr = (T*)st.data();
-    for (int k = 0; k < g.nbox; ++k)
-        for (unsigned yy = 0; yy < g.box[1]; ++yy)
-            for (unsigned xx = 0; xx < g.box[0]; ++xx) {
-                const unsigned long long y = (unsigned long long)k * g.box[1] + yy;
-                const T* src = (const T*)((const unsigned char*)a.in + (unsigned long long)z * g.stride_bytes[1] +
-                                          y * g.stride_bytes[0]) + x + xx;
-                nfft_emu_check(src, sizeof(T), 0);
-                sr[y * g.box[0] + xx] = *src;
-            }
-    // consumer phases
-    std::vector<LeanLine> lines(Lt::J);
-    for (int t = 0; t < Lt::J; ++t) {
-        long long bin, bout, j;
-        int i_;
-        resident_line(a, Lt::LOGJ, LOGR, gt, t, bin, bout, j, i_);
-        lines[t] = LeanLine{bin, bout, j};
-    }
-    if (a.discard_in)
-        for (int w = 0; w < ((Lt::J * (int)sizeof(V) / 128) << LOGR); ++w) {
-            const void* p = tma_discard_line<Lt, V>(a, gt, w);
-            if (p && ((uintptr_t)p & 127)) {
-                fprintf(stderr, "nfft_emu: discarded scratch line is not 128-byte aligned\n");
-                abort();
-            }
-            if (p) nfft_emu_check(p, 128, 0);
-        }
-    std::vector<V> regs((size_t)TH * 16);
-    std::vector<int> ls((size_t)TH * 16), is((size_t)TH * 16);
-    for (int t = 0; t < TH; ++t) tma_stage_read<Lt, V>(a, st.data(), t, &regs[t * 16], ls[t * 16], is[t * 16]);
-    for (int t = 0; t < TH; ++t) {
-        const int l = ls[t * 16], i = is[t * 16];
-        const long long j = ((gt << Lt::LOGJ) + l) & ((1ll << a.logNj) - 1);
-        Lt::pre_twiddle_dft(a, tw, j, i, &regs[t * 16]);
-        Lt::template write_smem<0>(st.data(), l, i, &regs[t * 16]);
-    }
-    auto middle = [&](auto Sc) {
-        constexpr int S = decltype(Sc)::value;
-        constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-        for (int t = 0; t < TH; ++t)
-            for (int q = 0; q < 16 / RHO; ++q)
-                Lt::template read<S, Lt::COLL>(st.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
-        for (int t = 0; t < TH; ++t)
-            for (int q = 0; q < 16 / RHO; ++q) {
-                Lt::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
-                Lt::template write_smem<S>(st.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
-            }
-    };
-    if constexpr (Lt::NS >= 3) middle(std::integral_constant<int, 1>{});
-    if constexpr (Lt::NS >= 4) middle(std::integral_constant<int, 2>{});
-    constexpr int S = Lt::NS - 1;
-    constexpr int RHO = 1 << LeanSched<LOGR>::lr[S];
-    for (int t = 0; t < TH; ++t)
-        for (int q = 0; q < 16 / RHO; ++q)
-            Lt::template read<S, Lt::COL_OUT_>(st.data(), t, q, &regs[t * 16 + q * RHO], ls[t * 16 + q], is[t * 16 + q]);
-    for (int t = 0; t < TH; ++t)
-        for (int q = 0; q < 16 / RHO; ++q) {
-            Lt::template twiddle_dft<S>(tw, is[t * 16 + q], &regs[t * 16 + q * RHO]);
-            Lt::template write_global<S>(a, tw, lines.data(), ls[t * 16 + q], is[t * 16 + q], &regs[t * 16 + q * RHO]);
-        }
-}
-
-typedef void (*EmuTmaTile)(const PassArgs&, long long, long long);
-static long long g_resident_tma_launches = 0;
-
-static bool emu_resident_tma(const ResidentTmaEntry* e, const PassArgs& a1, const PassArgs& a2, long long B) {
-    static std::map<std::pair<int, int>, std::pair<EmuTmaTile, EmuTmaTile>> fns = [] {
-        std::map<std::pair<int, int>, std::pair<EmuTmaTile, EmuTmaTile>> m;
-#define X(R1, R2, LT, NG)                                                                                         \
-    m[{R1, R2}] = {emu_tma_tile<TmaRes<real_t, R1, R2, LT>::L1, TmaRes<real_t, R1, R2, LT>::STAGE,                \
-                                TmaRes<real_t, R1, R2, LT>::TILE_BYTES>,                                          \
-                   emu_tma_tile<TmaRes<real_t, R1, R2, LT>::L2, TmaRes<real_t, R1, R2, LT>::STAGE,                \
-                                TmaRes<real_t, R1, R2, LT>::TILE_BYTES>};
-        NFFT_RESIDENT_TMA(X)
-#undef X
-        return m;
-    }();
-    if (e->stages <= e->ng || e->smem > 232448) {
-        fprintf(stderr, "nfft_emu: tensor-copy resident kernel %d x %d: %d stages for %d groups, %zu bytes\n", e->r1,
-                e->r2, e->stages, e->ng, e->smem);
-        abort();
-    }
-    const auto& f = fns[{e->r1, e->r2}];
-    const int lt = e->r1 + e->r2 - (e->logt + 4);
-    const long long T = 1ll << lt, lag = std::min<long long>(B, 2);
-    std::vector<long long> done((size_t)B, 0);
-    g_launches++;
-    g_resident_launches++;
-    g_resident_tma_launches++;
-    for (long long g = 0; g < 2 * B * T; ++g) {
-        int pass;
-        long long tr, tile;
-        resident_decode(g, B, lag, lt, pass, tr, tile);
-        if (pass == 2 && done[tr] != T) {
-            fprintf(stderr, "nfft_emu: resident pass-2 item %lld before its pass 1\n", g);
-            abort();
-        }
-        if (pass == 1) {
-            f.first(a1, (tr << lt) + tile, B);
-            done[tr]++;
-        } else {
-            f.second(a2, (tr << lt) + tile, B);
-        }
-    }
-    return true;
-}
-bool launch_resident(const DeviceCtx*, const PassArgs& a1, const PassArgs& a2, int r1, int r2, long long B,
-                     unsigned*, cudaStream_t) {
-    static std::map<std::pair<int, int>, std::pair<EmuLean, EmuLean>> fns = [] {
-        std::map<std::pair<int, int>, std::pair<EmuLean, EmuLean>> m;
-#define X(R1, R2, LT) \
-    m[{R1, R2}] = {emu_lean<R1, LT, true, false, LD_C, ST_C>, emu_lean<R2, LT, true, true, LD_C, ST_C>};
-        NFFT_RESIDENT_A(X) NFFT_RESIDENT_B(X)
-#undef X
-        return m;
-    }();
-    static const int mode = getenv("NOTORIOUS_FFT_RESIDENT") ? atoi(getenv("NOTORIOUS_FFT_RESIDENT")) : 0;
-    if (mode == 2)
-        if (const ResidentTmaEntry* te = resident_tma_find(r1, r2)) return emu_resident_tma(te, a1, a2, B);
-    const ResidentEntry* e = resident_find(r1, r2);
-    if (!e) {
-        set_error(6, "no resident kernel for radices 2^%d x 2^%d", r1, r2);
-        return false;
-    }
-    const auto& f = fns[{r1, r2}];
-    const int lt = r1 + r2 - (e->logt + 4);
-    const long long T = 1ll << lt, lag = std::min<long long>(B, 2);
-    std::vector<long long> done((size_t)B, 0);
-    g_launches++;
-    g_resident_launches++;
-    for (long long g = 0; g < 2 * B * T; ++g) {
-        int pass;
-        long long tr, tile;
-        resident_decode(g, B, lag, lt, pass, tr, tile);
-        if (tr < 0 || tr >= B || tile < 0 || tile >= T) {
-            fprintf(stderr, "nfft_emu: resident item %lld decodes outside the launch\n", g);
-            abort();
-        }
-        {
-            // the prefetching kernel's per-thread line and source addresses
-            const PassArgs& a = pass == 1 ? a1 : a2;
-            const int logR = pass == 1 ? r1 : r2, logJ = e->logt + 4 - logR;
-            const long long gt = (tr << lt) + tile;
-            for (int t = 0; t < (1 << e->logt); ++t) {
-                long long bin, bout, j, tmp[3];
-                int i;
-                resident_line(a, logJ, logR, gt, t, bin, bout, j, i);
-                TileLines tl{&tmp[0], &tmp[1], &tmp[2]};
-                line_setup(a, (gt << logJ) + (t & ((1 << logJ) - 1)), 0, tl);
-                if (bin != tmp[0] || bout != tmp[1] || j != tmp[2] || i != (t >> logJ)) {
-                    fprintf(stderr, "nfft_emu: resident line of thread %d differs from line_setup\n", t);
-                    abort();
-                }
-                const long long rs = a.in_estride << a.logNj;
-                const cplx_t* src = (const cplx_t*)a.in + bin + j * a.in_estride + (long long)i * rs;
-                for (int m = 0; m < 16; ++m) nfft_emu_check(src + m * (rs << (logR - 4)), sizeof(cplx_t), 0);
-            }
-        }
-        if (pass == 2) {
-            if (done[tr] != T) {
-                fprintf(stderr, "nfft_emu: resident pass-2 item %lld before its pass 1\n", g);
-                abort();
-            }
-            f.second(a2, (tr << lt) + tile, (tr << lt) + tile + 1);
-        } else {
-            f.first(a1, (tr << lt) + tile, (tr << lt) + tile + 1);
-            done[tr]++;
-        }
-    }
-    return true;
-}
-
 bool launch_post(cplx_t* post, long long n, cudaStream_t) {
     for (long long q = 0; q < n; ++q) {
         long double ang = 3.141592653589793238462643383279502884L * (long double)q / (long double)(2 * n);
@@ -1245,10 +818,6 @@ void nfft_emu_unregister_host(void* p) {
 }
 long long nfft_emu_launches(void) { return nfft::g_launches; }
 long long nfft_emu_lean_launches(void) { return nfft::g_lean_launches; }
-long long nfft_emu_cluster_launches(void) { return nfft::g_cluster_launches; }
 long long nfft_emu_checks(void) { return emu::n_checks; }
 long long nfft_emu_queue_items(void) { return nfft::g_queue_items; }
-long long nfft_emu_resident_launches(void) { return nfft::g_resident_launches; }
-long long nfft_emu_resident_tma_launches(void) { return nfft::g_resident_tma_launches; }
-long long nfft_emu_mid_launches(void) { return nfft::g_mid_launches; }
 }

@@ -253,31 +253,6 @@ def test_emu_pipelined_host_batches(emu_d, oracle_d):
 
 
 @pytest.mark.parametrize("single", [False, True])
-@pytest.mark.parametrize("n,batch", [(4097, 3), (40000, 2), (200003, 1)])
-def test_emu_bluestein_fused_middle(emu_d, emu_f, oracle_d, single, n, batch, monkeypatch):
-    """Multi-pass Bluestein (padded M = 2^14, 2^17, 2^19: middle radices 2^7,
-    2^8, 2^6) with NOTORIOUS_FFT_BLUE_MID=1 runs its last forward pass, filter
-    product and first inverse pass as one middle kernel; batched and inverse
-    transforms against the oracle."""
-    import ctypes
-    monkeypatch.setenv("NOTORIOUS_FFT_BLUE_MID", "1")
-    lib = emu_f if single else emu_d
-    f = lib.lib.nfft_emu_mid_launches
-    f.restype = ctypes.c_longlong
-    rng = np.random.default_rng(n)
-    x = (rng.uniform(-1, 1, (batch, n)) + 1j * rng.uniform(-1, 1, (batch, n))).astype(lib.cdt)
-    lim = (1e-6 if single else 1e-13) * np.log2(n)
-    m0 = f()
-    with lib.mkaux("dft", [n]) as a:
-        for k in ("dft", "invdft"):
-            y = np.zeros_like(x)
-            a.batched(k, x, y, batch, n, n)
-            for b in range(batch):
-                assert rel_l2(y[b], oracle_d.transform(k, x[b].astype(np.complex128))) <= lim, (k, b)
-    assert f() - m0 == 2
-
-
-@pytest.mark.parametrize("single", [False, True])
 @pytest.mark.parametrize("n", [64, 1024, 8192])
 def test_emu_real_rows_odd_batch_stride(emu_d, emu_f, oracle_d, n, single):
     """Batched single-pass real transforms whose input stride is odd: every other

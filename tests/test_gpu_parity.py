@@ -303,26 +303,6 @@ def test_split_tc_form_rejected_by_double_library(lib_d):
 
 
 @pytest.mark.parametrize("single", [False, True])
-@pytest.mark.parametrize("n,batch", [(4097, 5), (100003, 3), (1000003, 2)])
-def test_bluestein_fused_middle(lib_d, lib_f, oracle_d, single, n, batch, monkeypatch):
-    """The fused Bluestein middle (NOTORIOUS_FFT_BLUE_MID=1: last forward pass,
-    filter product and first inverse pass in one kernel) against the oracle."""
-    if single and n > 200000:
-        pytest.skip("float Bluestein checked up to 100,003 points")
-    monkeypatch.setenv("NOTORIOUS_FFT_BLUE_MID", "1")
-    lib = lib_f if single else lib_d
-    rng = np.random.default_rng(n)
-    x = (rng.uniform(-1, 1, (batch, n)) + 1j * rng.uniform(-1, 1, (batch, n))).astype(lib.cdt)
-    lim = (1e-6 if single else 1e-13) * np.log2(n)
-    with lib.mkaux("dft", [n]) as a:
-        for k in ("dft", "invdft"):
-            y = np.zeros_like(x)
-            a.batched(k, x, y, batch, n, n)
-            for b in (0, batch - 1):
-                assert rel_l2(y[b], oracle_d.transform(k, x[b].astype(np.complex128))) <= lim, (k, b)
-
-
-@pytest.mark.parametrize("single", [False, True])
 @pytest.mark.parametrize("n", [64, 4096, 16384])
 def test_real_rows_odd_batch_stride(lib_d, lib_f, oracle_d, single, n):
     """Batched single-pass real transforms with an odd input stride (every other
