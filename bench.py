@@ -15,7 +15,8 @@ Metric: HBM GB/s of algorithmic traffic (one read + one write of every
 transform's input and output, 2 N sizeof(cmpl) bytes per transform) on the
 device-resident batch, whole job (sum over GPUs).  `e2e` is the same metric
 through the C ABI with pinned host buffers (host<->device copies inside the
-timed region).  Multi-GPU runs shard the batch: every rank runs its own
+timed region); `e2e_pageable` the same calls on pageable host buffers (the
+library stages them through its own pinned buffers).  Multi-GPU runs shard the batch: every rank runs its own
 4096 transforms (weak scaling), no collective on the data path.
 """
 from __future__ import annotations
@@ -753,6 +754,7 @@ def main():
         configs = bench_configs(args, stream)
 
     e2e = None
+    e2e_pageable = None
     if not args.no_e2e and rank == 0 and world == 1:
         xh = x.cpu().pin_memory()
         yh = torch.empty_like(xh).pin_memory()
@@ -766,8 +768,25 @@ def main():
             aux.batched("invdft", yh, zh, B, N, N)
         dt = (time.perf_counter() - t0) / ks
         e2e = {"value": round(bytes_per_step / dt / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": 2 * B * N * 16,
-               "d2h_bytes_per_step": 2 * B * N * 16, "steps": ks, "timing": "host wall clock around synchronous C-ABI calls"}
+               "d2h_bytes_per_step": 2 * B * N * 16, "steps": ks, "timing": "host wall clock around synchronous C-ABI calls",
+               "host_memory": "pinned (page-locked)"}
         del xh, yh, zh
+        # the same calls on pageable host buffers (what a reference caller's
+        # malloc gives): staged through the library's pinned buffers
+        xp = x.cpu()
+        yp = torch.empty_like(xp)
+        zp = torch.empty_like(xp)
+        aux.batched("dft", xp, yp, B, N, N)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ks):
+            aux.batched("dft", xp, yp, B, N, N)
+            aux.batched("invdft", yp, zp, B, N, N)
+        dt = (time.perf_counter() - t0) / ks
+        e2e_pageable = {"value": round(bytes_per_step / dt / 1e9, 3), "unit": "GB/s",
+                        "h2d_bytes_per_step": 2 * B * N * 16, "d2h_bytes_per_step": 2 * B * N * 16, "steps": ks,
+                        "timing": "host wall clock around synchronous C-ABI calls", "host_memory": "pageable"}
+        del xp, yp, zp
 
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
@@ -788,7 +807,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (uniform[-1,1), torch seeded generator)",
             "config": {"workload": f"c2c fp64 N={N} x{B} dft+invdft per GPU", "N": N, "batch": B, "l2": wl["l2"],
                        "parallelism": f"batch-sharded x{world}"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_pageable": e2e_pageable, "gpu_launches": launches,
             "clocks": ck, "round_trip_rel_err": err,
         }
         line.update(forms)
