@@ -371,6 +371,10 @@ void* notorious_fft_get_stream(void) { return (void*)t_stream; }
 int notorious_fft_synchronize(void) {
     clear_error();
     if (!cuda_ok(cudaStreamSynchronize(t_stream), "cudaStreamSynchronize")) return last_error();
+    if (const unsigned st = tc_umma_take_status()) {
+        set_error(NOTORIOUS_FFT_ERR_CUDA, "tensor-core pass: wait %u gave up (results incomplete)", st);
+        return last_error();
+    }
     return 0;
 }
 

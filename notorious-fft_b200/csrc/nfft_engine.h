@@ -254,6 +254,14 @@ bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStrea
 // CTAs, nfft_tc_lean.cuh); NOTORIOUS_FFT_TC_LEAN=0 selects tc_pass_kernel.
 bool tc_lean_enabled();
 bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s);
+// The same passes on the sm_100 tensor cores (tcgen05, nfft_umma.cuh) for
+// unit-stride lines with 16-byte aligned buffers and strides; returns false
+// without launching (and without an error) when the pass is not of that
+// shape.  NOTORIOUS_FFT_TC_UMMA=0 keeps every pass on launch_tc_lean.
+bool tc_umma_enabled();
+bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& launched);
+// First wait of a tcgen05 pass that gave up since the last call (0: none), cleared.
+unsigned tc_umma_take_status();
 
 // Specialized pass kernels (nfft_lean.cuh), registered by the slice files.
 constexpr int NFFT_LEAN_SLICES = 8;

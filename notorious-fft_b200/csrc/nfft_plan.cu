@@ -440,11 +440,20 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
         rec->launches.push_back(r);
         return true;
     }
-    // split tensor-core form: radix-256 passes in the specialized kernel, other
-    // radices with the radix-16 sub-stages of the generic pass on the tensor cores
-    if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR == 8 && logNs + 8 <= 24 && tc_lean_enabled()) {
-        a.logJ = 4;
-        return launch_tc_lean(a, c->sm_count, s);
+    // split tensor-core form: radix-256 passes on tcgen05 where the layout
+    // allows (unit-stride lines, aligned strides), else in the warp-level
+    // specialized kernel; other radices with the radix-16 sub-stages of the
+    // generic pass on the tensor cores
+    if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR == 8 && logNs + 8 <= 24) {
+        if (tc_umma_enabled()) {
+            bool launched = false;
+            if (!try_launch_tc_umma(a, c->sm_count, s, launched)) return false;
+            if (launched) return true;
+        }
+        if (tc_lean_enabled()) {
+            a.logJ = 4;
+            return launch_tc_lean(a, c->sm_count, s);
+        }
     }
     if (op.tc && !mid && ldop == LD_C && stop == ST_C && logR >= 4 && tile == 12 && logJ == 12 - logR) {
         a.logJ = logJ;

@@ -1,8 +1,12 @@
 // nfft_tc.cu -- the split-tensor-core pass kernels of the float library
 // (NOTORIOUS_FFT_FORM_SPLIT_TC):
-//  * tc_lean_kernel: radix-256 passes, both radix-16 stages of a line as FP16
-//    hi + lo tensor-core products in registers (nfft_tc_lean.cuh), persistent
-//    CTAs over 16-line tiles -- every radix-256 pass of the form;
+//  * tc_umma_kernel: radix-256 passes on the sm_100 tensor cores (tcgen05
+//    products from shared memory into tensor memory, tensor copies in and
+//    out; nfft_umma.cuh) -- every radix-256 pass over unit-stride lines with
+//    16-byte aligned buffers and strides;
+//  * tc_lean_kernel: the other radix-256 passes, both radix-16 stages of a
+//    line as FP16 hi + lo warp-level products in registers
+//    (nfft_tc_lean.cuh), persistent CTAs over 16-line tiles;
 //  * tc_pass_kernel: the generic Stockham pass (nfft_pass.cuh) with its
 //    radix-16 sub-stages computed by tc_substage (nfft_tc.cuh) -- the other
 //    pass radices.
@@ -10,9 +14,12 @@
 
 #include <algorithm>
 
+#include <cuda.h>
+
 #include "nfft_engine.h"
 #include "nfft_tc.cuh"
 #include "nfft_tc_lean.cuh"
+#include "nfft_umma.cuh"
 
 namespace nfft {
 
@@ -173,6 +180,442 @@ bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s) {
     return cuda_ok(cudaGetLastError(), "tensor-core radix-256 pass launch");
 }
 
+// ---------------------------------------------------------------------------
+// Radix-256 passes on tcgen05 (layout: nfft_umma.cuh).  Persistent CTAs of
+// 128 threads, one tile (8 lines) at a time; the next tile's input copy runs
+// while the current one is transformed; thread t owns stage-1 row t and
+// stage-2 row t (line t >> 4), one thread issues the products.  Every wait
+// polls at most TcuArgs::spin times; a wait that gives up records 1 + its
+// kind in g_tcu_status, lets the copies and products in flight finish
+// (bounded), frees the tensor memory and leaves.
+// ---------------------------------------------------------------------------
+__device__ unsigned g_tcu_status;
+static bool s_tcu_used = false;   // a tcgen05 pass was launched in this process
+
+__device__ __forceinline__ uint32_t tcu_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// shared-memory matrix descriptor (sm_100): start, LBO, SBO (16-byte units), version 1, no swizzle
+__device__ __forceinline__ uint64_t tcu_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           ((uint64_t)1 << 46);
+}
+__device__ __forceinline__ bool tcu_try(uint64_t* m, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(tcu_smem(m)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool tcu_wait(uint64_t* m, unsigned parity, long long spin) {
+    for (long long n = 0; n < spin; ++n)
+        if (tcu_try(m, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tcu_load(const CUtensorMap* map, void* dst, uint64_t* bar, int c0, int c2) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tcu_smem(bar)), "r"(TCU_STAGE)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(tcu_smem(dst)),
+        "l"((uint64_t)map), "r"(c0), "r"(0), "r"(c2), "r"(tcu_smem(bar))
+        : "memory");
+}
+// D = Ah Bh + Al Bh + Ah Bl; K = 32 as two steps of 16 (two core matrices each)
+__device__ __forceinline__ void tcu_mma6(uint32_t d, uint32_t ah, uint32_t al, uint32_t bh, uint32_t bl) {
+    // instruction descriptor: FP32 accumulators, FP16 A and B, both K-major, N = 32, M = 128
+    const uint32_t idesc = (1u << 4) | ((uint32_t)(32 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    const uint32_t as[3] = {ah, al, ah}, bs[3] = {bh, bh, bl};
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            const uint64_t ad = tcu_desc(as[q] + ks * 2 * TCU_LBO, TCU_LBO, TCU_SBO);
+            const uint64_t bd = tcu_desc(bs[q] + ks * 2 * TCU_BLBO, TCU_BLBO, TCU_BSBO);
+            const uint32_t acc = (q | ks) ? 1u : 0u;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(d),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                : "memory");
+        }
+}
+__device__ __forceinline__ void tcu_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(tcu_smem(bar))
+                 : "memory");
+}
+// the 32 accumulator columns of this thread's row (warp w reads lanes 32 w ..)
+__device__ __forceinline__ void tcu_ld32(uint32_t taddr, float* v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]), "=f"(v[8]),
+          "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15]), "=f"(v[16]),
+          "=f"(v[17]), "=f"(v[18]), "=f"(v[19]), "=f"(v[20]), "=f"(v[21]), "=f"(v[22]), "=f"(v[23]), "=f"(v[24]),
+          "=f"(v[25]), "=f"(v[26]), "=f"(v[27]), "=f"(v[28]), "=f"(v[29]), "=f"(v[30]), "=f"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t tcu_h2(float re, float im) {
+    const __half2 h = __floats2half2_rn(re, im);
+    return *(const uint32_t*)&h;
+}
+// hi / lo FP16 parts of 4 complex points (scaled by sc), one 16-byte store each
+__device__ __forceinline__ void tcu_split4(unsigned char* hi, unsigned char* lo, int off, const float2* x, float sc) {
+    uint32_t hh[4], ll[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float re = x[q].x * sc, im = x[q].y * sc;
+        const __half2 h = __floats2half2_rn(re, im);
+        const float2 hf = __half22float2(h);
+        hh[q] = *(const uint32_t*)&h;
+        ll[q] = tcu_h2(re - hf.x, im - hf.y);
+    }
+    *(uint4*)(hi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+    *(uint4*)(lo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+}
+__device__ __forceinline__ float2 tcu_cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
+    tc_umma_kernel(const TcuArgs u, const __grid_constant__ CUtensorMap imap, const __grid_constant__ CUtensorMap omap) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    unsigned char* sm = smraw + ((512 - (tcu_smem(smraw) & 511)) & 511);
+    uint64_t* bar = (uint64_t*)(sm + TCU_OFF_BAR);   // [0] input tile, [1] products
+    uint32_t* tslot = (uint32_t*)(sm + TCU_OFF_BAR + 16);
+    const PassArgs& a = u.a;
+    const TwTables<float>* tw = (const TwTables<float>*)a.tw;
+    const int t = threadIdx.x, w = t >> 5;
+    const int l = t >> 4, i = t & 15;
+    const long long G = gridDim.x;
+    unsigned char* Ah = sm + TCU_OFF_AH;
+    unsigned char* Al = sm + TCU_OFF_AL;
+    // constants: the DFT matrix operands and the internal twiddles (with 2^-5)
+    for (int q = t; q < 32 * 32; q += TCU_THREADS) {
+        const int n = q >> 5, c = q & 31;
+        const float v = tcu_b_entry(tw, n, c);
+        const __half h = __float2half_rn(v);
+        const __half lo = __float2half_rn(v - __half2float(h));
+        const int off = tcu_b_off(n, c >> 1) + (c & 1) * 2;
+        *(__half*)(sm + TCU_OFF_BH + off) = h;
+        *(__half*)(sm + TCU_OFF_BL + off) = lo;
+    }
+    for (int q = t; q < 256; q += TCU_THREADS) {
+        const int ii = q >> 4, k1 = q & 15;
+        const C2<float> c = tw->t[0][(ii * k1 * 16) & (TW_SIZE - 1)];
+        const float f = tcu_pow2(-TCU_SCALE2);
+        ((float2*)(sm + TCU_OFF_TW))[k1 * 16 + ii] = make_float2(c.x * f, c.y * f);
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tcu_smem(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tcu_smem(&bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (w == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tcu_smem(tslot)),
+                     "r"(TCU_TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tbase = *tslot;
+    const uint32_t d1 = tbase, d2 = tbase + 32, lane_addr = (uint32_t)(32 * w) << 16;
+    const uint32_t ah = tcu_smem(Ah), al = tcu_smem(Al), bh = tcu_smem(sm + TCU_OFF_BH), bl = tcu_smem(sm + TCU_OFF_BL);
+    const float2* twt = (const float2*)(sm + TCU_OFF_TW);
+    const int logNs = a.logNs;
+    const float fscale = (float)a.scale;
+    bool pending = false;      // thread 0: an input copy in flight
+    bool mma_out = false;      // products whose completion was not observed (abandoned launch)
+    unsigned in_par = 0, mma_par = 0;
+    if (t == 0 && (long long)blockIdx.x < u.ntiles) {
+        const long long b = (long long)blockIdx.x / u.tiles_per_tr;
+        tcu_load(&imap, sm, &bar[0], (int)((long long)blockIdx.x - b * u.tiles_per_tr) * TCU_J, (int)b);
+        pending = true;
+    }
+    for (long long tile = blockIdx.x; tile < u.ntiles; tile += G) {
+        const bool got = tcu_wait(&bar[0], in_par, u.spin);
+        // the previous tile's output store has read its staging area
+        if (t == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        if (!__syncthreads_and(got)) {
+            if (t == 0) atomicCAS(&g_tcu_status, 0u, 1u);
+            break;
+        }
+        in_par ^= 1;
+        if (t == 0) pending = false;
+        long long b;
+        int j;
+        tcu_line(u, tile, t, b, j);
+        // ---- stage 1: row t = points i + 16 m of line l ----
+        float2 x[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) x[m] = *(const float2*)(sm + tcu_st_off(i + 16 * m, l));
+        if (a.conj_in) {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) x[m].y = -x[m].y;
+        }
+        if (logNs > 0) {
+            const long long k = j & ((1ll << logNs) - 1);
+            if (k) {
+                // W_{256 Ns}^{(i + 16 m) k} = W_{256 Ns}^{i k} (W_{16 Ns}^k)^m, powers by a depth-4 tree
+                const C2<float> wb0 = twiddle<float>(tw, (uint64_t)i * (uint64_t)k, logNs + 8);
+                const C2<float> st0 = twiddle<float>(tw, (uint64_t)k, logNs + 4);
+                const float2 wb = make_float2(wb0.x, wb0.y), s1 = make_float2(st0.x, st0.y);
+                float2 pw[16];
+                pw[0] = wb;
+                pw[1] = tcu_cmul(wb, s1);
+                const float2 s2 = tcu_cmul(s1, s1), s4 = tcu_cmul(s2, s2), s8 = tcu_cmul(s4, s4);
+                pw[2] = tcu_cmul(wb, s2);
+                pw[3] = tcu_cmul(pw[1], s2);
+#pragma unroll
+                for (int m = 4; m < 8; ++m) pw[m] = tcu_cmul(pw[m - 4], s4);
+#pragma unroll
+                for (int m = 8; m < 16; ++m) pw[m] = tcu_cmul(pw[m - 8], s8);
+#pragma unroll
+                for (int m = 0; m < 16; ++m) x[m] = tcu_cmul(x[m], pw[m]);
+            }
+        }
+        // one power-of-two scale per line (its 16 rows are 16 lanes of one warp)
+        float mx = 0.f;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) mx = fmaxf(mx, fmaxf(fabsf(x[m].x), fabsf(x[m].y)));
+#pragma unroll
+        for (int o = 1; o < 16; o <<= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        const int e1 = tcu_exp(mx);
+        const float s_in = tcu_pow2(-e1);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c], s_in);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();   // tile read, stage-1 operand written
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const long long next = tile + G;
+            if (next < u.ntiles) {
+                const long long nb = next / u.tiles_per_tr;
+                tcu_load(&imap, sm, &bar[0], (int)(next - nb * u.tiles_per_tr) * TCU_J, (int)nb);
+                pending = true;
+            }
+            tcu_mma6(d1, ah, al, bh, bl);
+            tcu_commit(&bar[1]);
+        }
+        bool ok = tcu_wait(&bar[1], mma_par, u.spin);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!__syncthreads_and(ok)) {
+            mma_out = true;
+            if (t == 0) atomicCAS(&g_tcu_status, 0u, 2u);
+            break;
+        }
+        mma_par ^= 1;
+        // ---- stage-1 outputs y[k1] of row t: twiddle, transpose into stage-2 rows 16 l + k1 ----
+        float v[32];
+        tcu_ld32(d1 + lane_addr, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const float2 c = twt[q * 16 + i];
+            const float re = v[2 * q] * c.x - v[2 * q + 1] * c.y;
+            const float im = v[2 * q] * c.y + v[2 * q + 1] * c.x;
+            const int off = tcu_a_off(16 * l + q, i);
+            const __half2 h = __floats2half2_rn(re, im);
+            const float2 hf = __half22float2(h);
+            *(__half2*)(Ah + off) = h;
+            *(uint32_t*)(Al + off) = tcu_h2(re - hf.x, im - hf.y);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            tcu_mma6(d2, ah, al, bh, bl);
+            tcu_commit(&bar[1]);
+        }
+        ok = tcu_wait(&bar[1], mma_par, u.spin);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!__syncthreads_and(ok)) {
+            mma_out = true;
+            if (t == 0) atomicCAS(&g_tcu_status, 0u, 3u);
+            break;
+        }
+        mma_par ^= 1;
+        // ---- stage-2 row t = 16 l + k1: outputs k1 + 16 k2 of line l, staged in the A region ----
+        tcu_ld32(d2 + lane_addr, v);
+        const float g = tcu_pow2(e1 + TCU_SCALE2) * fscale;
+        const float gi = a.conj_out ? -g : g;
+        unsigned char* ob = Ah;
+        if (u.out_kind == TCU_OUT_ROW) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                *(float2*)(ob + l * 2048 + (i + 16 * q) * 8) = make_float2(v[2 * q] * g, v[2 * q + 1] * gi);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                *(float2*)(ob + tcu_st_off(i + 16 * q, l)) = make_float2(v[2 * q] * g, v[2 * q + 1] * gi);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (t == 0) {
+            const int j0 = (int)(tile - b * u.tiles_per_tr) * TCU_J;
+            if (u.out_kind == TCU_OUT_ROW) {
+                asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                                 (uint64_t)&omap),
+                             "r"(0), "r"(j0), "r"((int)b), "r"(tcu_smem(ob))
+                             : "memory");
+            } else if (u.out_kind == TCU_OUT_COLSPLIT) {
+                const int lo = a.logNs_out;
+                asm volatile(
+                    "cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
+                        (uint64_t)&omap),
+                    "r"(j0 & ((1 << lo) - 1)), "r"(0), "r"(j0 >> lo), "r"((int)b), "r"(tcu_smem(ob))
+                    : "memory");
+            } else {
+                asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                                 (uint64_t)&omap),
+                             "r"(j0), "r"(0), "r"((int)b), "r"(tcu_smem(ob))
+                             : "memory");
+            }
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        if (mma_out) tcu_wait(&bar[1], mma_par, u.spin);   // abandoned launch: products still running
+        if (pending) tcu_wait(&bar[0], in_par, u.spin);    // abandoned launch: a copy still in flight
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (w == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TCU_TCOLS) : "memory");
+}
+
+bool tc_umma_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NOTORIOUS_FFT_TC_UMMA");
+        v = e ? atoi(e) : 1;
+    }
+    return v != 0;
+}
+
+typedef CUresult (*TcuEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static TcuEncodeFn tcu_encoder() {
+    static TcuEncodeFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (TcuEncodeFn)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Tensor map of 8-byte elements (one complex float); strides in bytes.
+static bool tcu_map(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
+                    const cuuint32_t* box, CUtensorMapSwizzle sw) {
+    TcuEncodeFn enc = tcu_encoder();
+    if (!enc) return false;
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)rank, const_cast<void*>(base), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& launched) {
+    launched = false;
+    // the shape this kernel covers: lines j of a transform at unit stride,
+    // one batch dimension, plain complex loads and stores, 16-byte aligned
+    if (a.logR != 8 || a.ndims != 2 || a.jpos != 0 || a.in_estride != 1 || a.out_estride != 1) return true;
+    if (a.in_tab || a.out_tab || a.mid || a.vjp || a.logNj < 3 || a.cnt[0] != (1ll << a.logNj)) return true;
+    if (a.logNs_out != 0 && a.logNs_out < 3) return true;
+    if (((uintptr_t)a.in & 15) || ((uintptr_t)a.out & 15) || a.in == a.out) return true;
+    const long long B = a.cnt[1], Nj = a.cnt[0];
+    if (B < 1 || Nj * B != a.nlines) return true;
+    if (B > 1 && ((a.istr[1] & 1) || (a.ostr[1] & 1) || a.istr[1] <= 0 || a.ostr[1] <= 0)) return true;
+    const long long istr = B > 1 ? a.istr[1] * 8 : Nj * 256 * 8;
+    const long long ostr = B > 1 ? a.ostr[1] * 8 : Nj * 256 * 8;
+    CUtensorMap imap, omap;
+    {
+        const cuuint64_t dims[3] = {(cuuint64_t)Nj, 256, (cuuint64_t)B};
+        const cuuint64_t strides[2] = {(cuuint64_t)(Nj * 8), (cuuint64_t)istr};
+        const cuuint32_t box[3] = {TCU_J, 256, 1};
+        if (!tcu_map(&imap, a.in, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_64B)) return true;
+    }
+    const int so = a.logNs_out;
+    int kind;
+    if (so == 0) {
+        kind = TCU_OUT_ROW;
+        const cuuint64_t dims[3] = {256, (cuuint64_t)Nj, (cuuint64_t)B};
+        const cuuint64_t strides[2] = {2048, (cuuint64_t)ostr};
+        const cuuint32_t box[3] = {256, TCU_J, 1};
+        if (!tcu_map(&omap, a.out, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_NONE)) return true;
+    } else if (so < a.logNj) {
+        kind = TCU_OUT_COLSPLIT;
+        const cuuint64_t dims[4] = {(cuuint64_t)1 << so, 256, (cuuint64_t)(Nj >> so), (cuuint64_t)B};
+        const cuuint64_t strides[3] = {(cuuint64_t)8 << so, (cuuint64_t)8 << (so + 8), (cuuint64_t)ostr};
+        const cuuint32_t box[4] = {TCU_J, 256, 1, 1};
+        if (!tcu_map(&omap, a.out, 4, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_64B)) return true;
+    } else {
+        kind = TCU_OUT_COL;
+        const cuuint64_t dims[3] = {(cuuint64_t)Nj, 256, (cuuint64_t)B};
+        const cuuint64_t strides[2] = {(cuuint64_t)8 << so, (cuuint64_t)ostr};
+        const cuuint32_t box[3] = {TCU_J, 256, 1};
+        if (!tcu_map(&omap, a.out, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_64B)) return true;
+    }
+    static bool attr = false;
+    if (!attr) {
+        if (!cuda_ok(cudaFuncSetAttribute((const void*)tc_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          TCU_SMEM),
+                     "cudaFuncSetAttribute(tc umma)"))
+            return false;
+        if (!cuda_ok(cudaFuncSetAttribute((const void*)tc_umma_kernel,
+                                          cudaFuncAttributePreferredSharedMemoryCarveout, 100),
+                     "cudaFuncSetAttribute(tc umma carveout)"))
+            return false;
+        attr = true;
+    }
+    TcuArgs u;
+    u.a = a;
+    u.out_kind = kind;
+    u.tiles_per_tr = Nj / TCU_J;
+    u.ntiles = u.tiles_per_tr * B;
+    u.status = nullptr;
+    u.spin = 1ll << 22;
+    // resident CTAs: shared memory and registers allow TCU_MINB per SM
+    // (the occupancy query does not count kernels that allocate tensor memory)
+    const long long grid = std::min<long long>(u.ntiles, (long long)std::max(sm_count, 1) * TCU_MINB);
+    if (grid <= 0) {
+        launched = true;
+        return true;
+    }
+    tc_umma_kernel<<<(unsigned)grid, TCU_THREADS, TCU_SMEM, s>>>(u, imap, omap);
+    note_launch();
+    s_tcu_used = true;
+    launched = true;
+    return cuda_ok(cudaGetLastError(), "tensor-core (tcgen05) radix-256 pass launch");
+}
+
+unsigned tc_umma_take_status() {
+    if (!s_tcu_used) return 0;
+    unsigned v = 0, z = 0;
+    if (cudaMemcpyFromSymbol(&v, g_tcu_status, sizeof v) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (v) cudaMemcpyToSymbol(g_tcu_status, &z, sizeof z);
+    return v;
+}
+
 bool launch_tc_pass(const PassArgs& a, int log_tile, long long ntiles, cudaStream_t s) {
     static bool attr = false;
     const size_t smem = pass_smem_bytes<float>(log_tile);
@@ -201,6 +644,15 @@ bool launch_tc_lean(const PassArgs&, int, cudaStream_t) {
     set_error(6, "the split tensor-core form exists in the float library only");
     return false;
 }
+
+bool tc_umma_enabled() { return false; }
+
+bool try_launch_tc_umma(const PassArgs&, int, cudaStream_t, bool& launched) {
+    launched = false;
+    return true;
+}
+
+unsigned tc_umma_take_status() { return 0; }
 
 bool launch_tc_pass(const PassArgs&, int, long long, cudaStream_t) {
     set_error(6, "the split tensor-core form exists in the float library only");

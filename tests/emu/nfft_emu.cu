@@ -627,6 +627,15 @@ static void emu_tcl_stage(const TcA* A, uint32_t (*xb)[2][2][2][2], float (*acc)
         }
 }
 
+// The tcgen05 radix-256 pass has no CPU model here: emulated runs take the
+// warp-level kernel's path for every radix-256 pass of the split form.
+bool tc_umma_enabled() { return false; }
+bool try_launch_tc_umma(const PassArgs&, int, cudaStream_t, bool& launched) {
+    launched = false;
+    return true;
+}
+unsigned tc_umma_take_status() { return 0; }
+
 bool tc_lean_enabled() {
     const char* e = getenv("NOTORIOUS_FFT_TC_LEAN");
     return !e || atoi(e) != 0;
