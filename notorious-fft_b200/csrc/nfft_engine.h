@@ -127,6 +127,10 @@ struct notorious_fft_plan {
     // pipelined host-pointer calls: copy streams, events, double-buffered staging
     cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
     cudaEvent_t ev_h[2] = {nullptr, nullptr}, ev_c[2] = {nullptr, nullptr}, ev_d[2] = {nullptr, nullptr};
+    // pageable host calls: pinned host bounce buffers of the chunks in flight
+    void* host_in = nullptr;
+    void* host_out = nullptr;
+    size_t host_in_bytes = 0, host_out_bytes = 0;
     // temporary of the multi-dimensional inverse real transform
     void* nd_tmp = nullptr;
     size_t nd_tmp_bytes = 0;

@@ -846,6 +846,8 @@ void plan_destroy(notorious_fft_plan* p) {
     if (p->s_d2h) cudaStreamDestroy(p->s_d2h);
     if (p->nd_tmp) cudaFree(p->nd_tmp);
     if (p->stage_out) cudaFree(p->stage_out);
+    if (p->host_in) cudaFreeHost(p->host_in);
+    if (p->host_out) cudaFreeHost(p->host_out);
     if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
     delete p;
 }

@@ -6,7 +6,10 @@
   streams).  The batches here span at least three chunks, in both
   libraries, out of place, in place (x == y) and with odd distances.  The
   reference's own callers pass host pointers (benchmarks/bench.c:35-55).
-* Pageable host buffers take the staged path (one copy in, one copy out).
+* Pageable host buffers on a batch of >= 4 transforms take the same chunked
+  pipeline with pinned bounce buffers filled and drained by host threads
+  (csrc/nfft_api.cu run_pageable_pipelined); smaller batches the staged path
+  (one copy in, one copy out).
 * Two device-pointer calls on one aux from two streams: the plan's scratch is
   shared, so the second call waits for the first (csrc/nfft_api.cu
   order_after_previous_call); both results must match the oracle.
@@ -93,6 +96,34 @@ def test_pipelined_realdft_odd_distance(lib_d, lib_f, oracle_d, single):
         w = g[b * odist:(b + 1) * odist].astype(np.complex128)
         w[1:-1] *= 0.5
         assert rel_l2(gxh[b * n:(b + 1) * n], oracle_d.invrealdft(w, n)) <= tol, b
+
+
+@pytest.mark.parametrize("single", [False, True], ids=["double", "float"])
+@pytest.mark.parametrize("in_place", [False, True], ids=["out-of-place", "in-place"])
+def test_pageable_pipelined_c2c(lib_d, lib_f, oracle_d, single, in_place):
+    """Pageable numpy buffers over more than three 64 MiB chunks, odd distances."""
+    lib = lib_f if single else lib_d
+    es = 8 if single else 16
+    n = 4096
+    idist = n + 3
+    batch = 3 * (64 << 20) // (idist * es) + 7
+    rng = np.random.default_rng(batch + 1)
+    x = (rng.uniform(-1, 1, batch * idist) + 1j * rng.uniform(-1, 1, batch * idist)).astype(lib.cdt)
+    x0 = x.copy()
+    if in_place:
+        y, odist = x, idist
+    else:
+        odist = n + 1
+        y = np.full(batch * odist, np.nan, lib.cdt)
+    with lib.mkaux("dft", [n]) as a:
+        a.batched("dft", x, y, batch, idist, odist)
+    tol = _tol(n, single)
+    for b in _sample(batch):
+        ref = oracle_d.transform("dft", x0[b * idist: b * idist + n].astype(np.complex128))
+        assert rel_l2(y[b * odist: b * odist + n], ref) <= tol, b
+    xb = np.lib.stride_tricks.as_strided(x0, (batch, n), (idist * x0.itemsize, x0.itemsize))
+    yb = np.lib.stride_tricks.as_strided(y, (batch, n), (odist * y.itemsize, y.itemsize))
+    assert rel_l2(yb, np.fft.fft(xb.astype(np.complex128), axis=1)) <= tol
 
 
 def test_pageable_host_batched_dct2(lib_d, oracle_d):
