@@ -259,12 +259,12 @@ __device__ __forceinline__ uint32_t tcu_h2(float re, float im) {
     const __half2 h = __floats2half2_rn(re, im);
     return *(const uint32_t*)&h;
 }
-// hi / lo FP16 parts of 4 complex points (scaled by sc), one 16-byte store each
-__device__ __forceinline__ void tcu_split4(unsigned char* hi, unsigned char* lo, int off, const float2* x, float sc) {
+// hi / lo FP16 parts of 4 complex points, one 16-byte store each
+__device__ __forceinline__ void tcu_split4(unsigned char* hi, unsigned char* lo, int off, const float2* x) {
     uint32_t hh[4], ll[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const float re = x[q].x * sc, im = x[q].y * sc;
+        const float re = x[q].x, im = x[q].y;
         const __half2 h = __floats2half2_rn(re, im);
         const float2 hf = __half22float2(h);
         hh[q] = *(const uint32_t*)&h;
@@ -303,8 +303,7 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     for (int q = t; q < 256; q += TCU_THREADS) {
         const int ii = q >> 4, k1 = q & 15;
         const C2<float> c = tw->t[0][(ii * k1 * 16) & (TW_SIZE - 1)];
-        const float f = tcu_pow2(-TCU_SCALE2);
-        ((float2*)(sm + TCU_OFF_TW))[k1 * 16 + ii] = make_float2(c.x * f, c.y * f);
+        ((float2*)(sm + TCU_OFF_TW))[k1 * 16 + ii] = make_float2(c.x, c.y);
     }
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tcu_smem(&bar[0])) : "memory");
@@ -377,16 +376,24 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
                 for (int m = 0; m < 16; ++m) x[m] = tcu_cmul(x[m], pw[m]);
             }
         }
-        // one power-of-two scale per line (its 16 rows are 16 lanes of one warp)
+        // one power-of-two scale per line (its 16 rows are 16 lanes of one warp),
+        // none when the line's largest component is already in the unscaled range
         float mx = 0.f;
 #pragma unroll
         for (int m = 0; m < 16; ++m) mx = fmaxf(mx, fmaxf(fabsf(x[m].x), fabsf(x[m].y)));
 #pragma unroll
         for (int o = 1; o < 16; o <<= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        const int e1 = tcu_exp(mx);
-        const float s_in = tcu_pow2(-e1);
+        const int e1 = (mx >= TCU_LO && mx < TCU_HI) ? 0 : tcu_exp(mx);
+        if (e1 == 0) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c], s_in);
+            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c]);
+        } else {
+            const float s_in = tcu_pow2(-e1);
+#pragma unroll
+            for (int m = 0; m < 16; ++m) x[m] = make_float2(x[m].x * s_in, x[m].y * s_in);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c]);
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();   // tile read, stage-1 operand written
@@ -441,17 +448,24 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         mma_par ^= 1;
         // ---- stage-2 row t = 16 l + k1: outputs k1 + 16 k2 of line l, staged in the A region ----
         tcu_ld32(d2 + lane_addr, v);
-        const float g = tcu_pow2(e1 + TCU_SCALE2) * fscale;
+        const float g = tcu_pow2(e1) * fscale;
         const float gi = a.conj_out ? -g : g;
+        if (g != 1.f || gi != 1.f) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                v[2 * q] *= g;
+                v[2 * q + 1] *= gi;
+            }
+        }
         unsigned char* ob = Ah;
         if (u.out_kind == TCU_OUT_ROW) {
 #pragma unroll
             for (int q = 0; q < 16; ++q)
-                *(float2*)(ob + l * 2048 + (i + 16 * q) * 8) = make_float2(v[2 * q] * g, v[2 * q + 1] * gi);
+                *(float2*)(ob + l * 2048 + (i + 16 * q) * 8) = make_float2(v[2 * q], v[2 * q + 1]);
         } else {
 #pragma unroll
             for (int q = 0; q < 16; ++q)
-                *(float2*)(ob + tcu_st_off(i + 16 * q, l)) = make_float2(v[2 * q] * g, v[2 * q + 1] * gi);
+                *(float2*)(ob + tcu_st_off(i + 16 * q, l)) = make_float2(v[2 * q], v[2 * q + 1]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -8,12 +8,11 @@
 // issued by one thread as tcgen05.mma with the operands in shared memory and
 // the accumulators in tensor memory:
 //  * stage 1: row t = 16 l + i holds the 16 points i + 16 m of line l
-//    (pass pre-twiddled, scaled by the line's power of two), columns
+//    (pass pre-twiddled, scaled by a power of two when out of range), columns
 //    (2m, 2m+1) = (re, im); B is the real form of the radix-16 DFT matrix;
 //    D row t = y_{l,i}[k1];
-//  * the internal twiddles W_256^{i k1} (carrying 2^-5, so stage-2 inputs
-//    stay below 2 in modulus: |y| <= 16 * 2 * sqrt(2) < 2^6 times the line
-//    scale), transposed into stage-2 rows 16 l + k1, columns (2i, 2i+1);
+//  * the internal twiddles W_256^{i k1}, transposed into stage-2 rows
+//    16 l + k1, columns (2i, 2i+1);
 //  * stage 2 rows: z_{l,k1}[k2] = output point k1 + 16 k2 of line l.
 // A operand layout: K-major, no swizzle: 8-row x 16-byte core matrices at
 // row-group stride TCU_SBO and K-chunk stride TCU_LBO (padded so both the
@@ -38,11 +37,17 @@ constexpr int TCU_OFF_AH = TCU_STAGE;
 constexpr int TCU_OFF_AL = TCU_OFF_AH + TCU_AOP;
 constexpr int TCU_OFF_BH = TCU_OFF_AL + TCU_AOP;
 constexpr int TCU_OFF_BL = TCU_OFF_BH + TCU_BOP;
-constexpr int TCU_OFF_TW = TCU_OFF_BL + TCU_BOP;   // W_256^{i k1} 2^-5, stored [k1][i]
+constexpr int TCU_OFF_TW = TCU_OFF_BL + TCU_BOP;   // W_256^{i k1}, stored [k1][i]
 constexpr int TCU_OFF_BAR = TCU_OFF_TW + 256 * 8;  // mbarriers and the tensor-memory address
 constexpr int TCU_SMEM = TCU_OFF_BAR + 64 + 512;   // + alignment of the stage to 512 bytes
 constexpr int TCU_TCOLS = 64;                      // stage-1 and stage-2 accumulators
-constexpr int TCU_SCALE2 = 5;
+// Range: a radix-16 output is at most 16 sqrt(2) times the largest input
+// component in modulus, so a line whose largest component is below 2^8 keeps
+// every stage-1 output, stage-2 operand (< 5800) and FP16 part within FP16
+// range; from 1/2 up the lo parts of its large values stay normal FP16
+// numbers.  Lines outside [TCU_LO, TCU_HI) are scaled by a power of two into
+// [1, 2) before the split and unscaled exactly after stage 2.
+constexpr float TCU_LO = 0.5f, TCU_HI = 256.f;
 
 // Where a pass writes: row out (Ns = 1, line j's outputs contiguous), column
 // out with j split at Ns (Ns < lines), column out (Ns >= lines).
