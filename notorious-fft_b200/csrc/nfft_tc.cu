@@ -185,9 +185,10 @@ bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s) {
 // 128 threads, one tile (8 lines) at a time; the next tile's input copy runs
 // while the current one is transformed; thread t owns stage-1 row t and
 // stage-2 row t (line t >> 4), one thread issues the products.  Every wait
-// polls at most TcuArgs::spin times; a wait that gives up records 1 + its
-// kind in g_tcu_status, lets the copies and products in flight finish
-// (bounded), frees the tensor memory and leaves.
+// polls at most TcuArgs::spin times and at most 2 s; a wait that gives up
+// records its kind (1: input copy, 2 / 3: stage-1 / stage-2 products) in
+// g_tcu_status, lets the copies and products in flight finish (bounded),
+// frees the tensor memory and leaves.
 // ---------------------------------------------------------------------------
 __device__ unsigned g_tcu_status;
 static bool s_tcu_used = false;   // a tcgen05 pass was launched in this process
@@ -206,9 +207,20 @@ __device__ __forceinline__ bool tcu_try(uint64_t* m, unsigned parity) {
                  : "memory");
     return ok != 0;
 }
+__device__ __forceinline__ uint64_t tcu_now() {
+    uint64_t v;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+    return v;
+}
+// At most `spin` polls and at most 2 s (a poll may suspend the thread for a
+// system-dependent time).
 __device__ __forceinline__ bool tcu_wait(uint64_t* m, unsigned parity, long long spin) {
-    for (long long n = 0; n < spin; ++n)
+    if (tcu_try(m, parity)) return true;
+    const uint64_t t0 = tcu_now();
+    for (long long n = 1; n < spin; ++n) {
         if (tcu_try(m, parity)) return true;
+        if ((n & 255) == 0 && tcu_now() - t0 > 2000000000ull) return false;
+    }
     return false;
 }
 __device__ __forceinline__ void tcu_load(const CUtensorMap* map, void* dst, uint64_t* bar, int c0, int c2) {
@@ -329,7 +341,7 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     bool pending = false;      // thread 0: an input copy in flight
     bool mma_out = false;      // products whose completion was not observed (abandoned launch)
     unsigned in_par = 0, mma_par = 0;
-    if (t == 0 && (long long)blockIdx.x < u.ntiles) {
+    if (t == 0 && (long long)blockIdx.x < u.ntiles && !u.withhold) {
         const long long b = (long long)blockIdx.x / u.tiles_per_tr;
         tcu_load(&imap, sm, &bar[0], (int)((long long)blockIdx.x - b * u.tiles_per_tr) * TCU_J, (int)b);
         pending = true;
@@ -604,7 +616,19 @@ bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& l
     u.tiles_per_tr = Nj / TCU_J;
     u.ntiles = u.tiles_per_tr * B;
     u.status = nullptr;
-    u.spin = 1ll << 22;
+    // NOTORIOUS_FFT_TC_UMMA_SPIN / _WITHHOLD: the failure test's short poll limit
+    // and a first input copy that is never issued (every CTA's first wait runs out)
+    static const long long spin = [] {
+        const char* e = getenv("NOTORIOUS_FFT_TC_UMMA_SPIN");
+        const long long v = e ? atoll(e) : 0;
+        return v > 0 ? v : (1ll << 22);
+    }();
+    static const int withhold = [] {
+        const char* e = getenv("NOTORIOUS_FFT_TC_UMMA_WITHHOLD");
+        return e ? atoi(e) : 0;
+    }();
+    u.spin = spin;
+    u.withhold = withhold;
     // resident CTAs: shared memory and registers allow TCU_MINB per SM
     // (the occupancy query does not count kernels that allocate tensor memory)
     const long long grid = std::min<long long>(u.ntiles, (long long)std::max(sm_count, 1) * TCU_MINB);

@@ -60,6 +60,7 @@ struct TcuArgs {
     long long ntiles;
     unsigned* status;          // 1 + which wait gave up (0: none)
     long long spin;            // poll limit of every wait
+    int withhold;              // failure test: the first input copy is never issued
 };
 
 // point (row r, line l) of a 64-byte swizzled tile row (8 lines x 8 bytes)

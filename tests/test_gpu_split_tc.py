@@ -109,3 +109,47 @@ def test_split_tc_tcgen05_and_warp_kernels_agree(tmp_path, oracle_d):
     for mode, y in outs.items():
         assert max(rel_l2(y[b], ref[b]) for b in range(B)) <= 2e-6, mode
     assert max(rel_l2(outs["1"][b], outs["0"][b]) for b in range(B)) <= 2e-6
+
+
+WITHHOLD_CHILD = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, "notorious-fft_b200")
+sys.path.insert(0, "oracle")
+from notorious_fft import load, FORM_SPLIT_TC, NotoriousFFTError
+from oracle import Oracle, rel_l2
+F = load(single=True)
+n, B = 65536, 2
+x = torch.ones(B * n, dtype=torch.complex64, device="cuda")
+y = torch.empty_like(x)
+raised = False
+with F.mkaux("dft", [n]) as a:
+    a.set_form(FORM_SPLIT_TC)
+    a.batched("dft", x, y, B, n, n)
+    try:
+        F.synchronize()
+    except NotoriousFFTError as e:
+        raised = "gave up" in str(e)
+print("raised", raised)
+# the context stays usable: a double-library transform against the oracle
+D = load(single=False)
+rng = np.random.default_rng(1)
+xd = rng.uniform(-1, 1, (4, 4096)) + 1j * rng.uniform(-1, 1, (4, 4096))
+with D.mkaux("dft", [4096]) as a:
+    yd = a("dft", xd[0])
+print("after", rel_l2(yd, Oracle().transform("dft", xd[0])))
+"""
+
+
+def test_split_tc_wait_gives_up_and_reports():
+    """Failure detection of the tcgen05 pass without a GPU fault: with the first
+    input copy withheld (NOTORIOUS_FFT_TC_UMMA_WITHHOLD=1) every CTA's first
+    wait runs out after a short poll limit, the kernel frees its tensor memory
+    and returns, notorious_fft_synchronize reports the wait, and the context
+    still runs transforms correctly."""
+    env = dict(os.environ, NOTORIOUS_FFT_TC_UMMA_WITHHOLD="1", NOTORIOUS_FFT_TC_UMMA_SPIN="2000")
+    r = subprocess.run([sys.executable, "-c", WITHHOLD_CHILD], cwd=ROOT, env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = dict(l.split(" ", 1) for l in r.stdout.strip().splitlines() if " " in l)
+    assert lines.get("raised") == "True", r.stdout
+    assert float(lines["after"]) <= 1e-13 * 12, r.stdout
