@@ -60,6 +60,17 @@ bool is_pinned_host_ptr(const void* ptr) {
 // 16 threads: 4 / 8 / 12 / 16 threads gave 19 / 26 / 31 / 35 GB/s end to end on
 // 4096 x 2^16 FP64 dft + invdft, against 9.7 GB/s through the driver's own
 // staging of pageable memory).
+// Input bytes per chunk of the host-pointer pipelines (NOTORIOUS_FFT_PIPE_CHUNK_MB).
+size_t pipe_chunk_bytes() {
+    static size_t v = 0;
+    if (!v) {
+        const char* e = getenv("NOTORIOUS_FFT_PIPE_CHUNK_MB");
+        const long long mb = e ? atoll(e) : 64;
+        v = (size_t)std::max(1ll, std::min(mb, 4096ll)) << 20;
+    }
+    return v;
+}
+
 int host_copy_threads() {
     static int v = 0;
     if (!v) {
@@ -122,7 +133,7 @@ bool ensure_copy_streams(notorious_fft_plan* p) {
 bool run_pageable_pipelined(notorious_fft_plan* p, int kind, const void* x, void* y, long long howmany,
                             long long idist, long long odist, long long in_elems, long long out_elems, size_t in_eb,
                             size_t out_eb, int vjp, cudaStream_t s) {
-    const size_t target = (size_t)64 << 20;
+    const size_t target = pipe_chunk_bytes();
     long long chunk = (long long)(target / std::max<size_t>((size_t)idist * in_eb, 1));
     if (chunk < 1) chunk = 1;
     if (chunk > howmany) chunk = howmany;
@@ -188,7 +199,7 @@ bool run_pageable_pipelined(notorious_fft_plan* p, int kind, const void* x, void
 bool run_pipelined(notorious_fft_plan* p, int kind, const void* x, void* y, long long howmany, long long idist,
                    long long odist, long long in_elems, long long out_elems, size_t in_eb, size_t out_eb, int vjp,
                    cudaStream_t s) {
-    const size_t target = (size_t)64 << 20;
+    const size_t target = pipe_chunk_bytes();
     long long chunk = (long long)(target / std::max<size_t>((size_t)idist * in_eb, 1));
     if (chunk < 1) chunk = 1;
     if (chunk > howmany) chunk = howmany;
