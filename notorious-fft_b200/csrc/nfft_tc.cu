@@ -615,7 +615,6 @@ bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& l
     u.out_kind = kind;
     u.tiles_per_tr = Nj / TCU_J;
     u.ntiles = u.tiles_per_tr * B;
-    u.status = nullptr;
     // NOTORIOUS_FFT_TC_UMMA_SPIN / _WITHHOLD: the failure test's short poll limit
     // and a first input copy that is never issued (every CTA's first wait runs out)
     static const long long spin = [] {

@@ -58,7 +58,6 @@ struct TcuArgs {
     int out_kind;
     long long tiles_per_tr;    // lines per transform / 8
     long long ntiles;
-    unsigned* status;          // 1 + which wait gave up (0: none)
     long long spin;            // poll limit of every wait
     int withhold;              // failure test: the first input copy is never issued
 };
