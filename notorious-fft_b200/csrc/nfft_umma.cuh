@@ -1,7 +1,6 @@
 // nfft_umma.cuh -- layout of the split tensor-core radix-256 pass on the
 // sm_100 tensor cores (tcgen05): the tile of 8 Stockham lines x 256 points,
-// its shared-memory operands and the index maps the kernel (nfft_tc.cu) and
-// its CPU model (tests/emu) share.
+// its shared-memory operands and the index maps of the kernel (nfft_tc.cu).
 //
 // Both radix-16 stages of the tile are 128 x 32 x 32 real products
 //     D = A_hi B_hi + A_lo B_hi + A_hi B_lo      (FP16 operands, FP32 sums)
