@@ -233,7 +233,7 @@ __device__ __forceinline__ void tcu_load(const CUtensorMap* map, void* dst, uint
         : "memory");
 }
 // D = Ah Bh + Al Bh + Ah Bl; K = 32 as two steps of 16 (two core matrices each)
-__device__ __forceinline__ void tcu_mma6(uint32_t d, uint32_t ah, uint32_t al, uint32_t bh, uint32_t bl) {
+__device__ __forceinline__ void tcu_mma6(uint32_t d, uint32_t ah, uint32_t al, uint32_t bh, uint32_t bl, uint32_t sbo) {
     // instruction descriptor: FP32 accumulators, FP16 A and B, both K-major, N = 32, M = 128
     const uint32_t idesc = (1u << 4) | ((uint32_t)(32 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
     const uint32_t as[3] = {ah, al, ah}, bs[3] = {bh, bh, bl};
@@ -241,7 +241,7 @@ __device__ __forceinline__ void tcu_mma6(uint32_t d, uint32_t ah, uint32_t al, u
     for (int q = 0; q < 3; ++q)
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
-            const uint64_t ad = tcu_desc(as[q] + ks * 2 * TCU_LBO, TCU_LBO, TCU_SBO);
+            const uint64_t ad = tcu_desc(as[q] + ks * 2 * TCU_LBO, TCU_LBO, sbo);
             const uint64_t bd = tcu_desc(bs[q] + ks * 2 * TCU_BLBO, TCU_BLBO, TCU_BSBO);
             const uint32_t acc = (q | ks) ? 1u : 0u;
             asm volatile(
@@ -285,9 +285,6 @@ __device__ __forceinline__ void tcu_split4(unsigned char* hi, unsigned char* lo,
     *(uint4*)(hi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
     *(uint4*)(lo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
 }
-__device__ __forceinline__ float2 tcu_cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
 
 __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     tc_umma_kernel(const TcuArgs u, const __grid_constant__ CUtensorMap imap, const __grid_constant__ CUtensorMap omap) {
@@ -298,7 +295,11 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     const PassArgs& a = u.a;
     const TwTables<float>* tw = (const TwTables<float>*)a.tw;
     const int t = threadIdx.x, w = t >> 5;
-    const int l = t >> 4, i = t & 15;
+    int l, i, l2, k2r;
+    tcu_role_a(t, l, i);
+    tcu_role_b(u.out_kind, t, l2, k2r);
+    const bool rowk = u.out_kind == TCU_OUT_ROW;
+    const int sbo = rowk ? TCU_SBO_ROW : TCU_SBO_COL;
     const long long G = gridDim.x;
     unsigned char* Ah = sm + TCU_OFF_AH;
     unsigned char* Al = sm + TCU_OFF_AL;
@@ -342,8 +343,10 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     bool mma_out = false;      // products whose completion was not observed (abandoned launch)
     unsigned in_par = 0, mma_par = 0;
     if (t == 0 && (long long)blockIdx.x < u.ntiles && !u.withhold) {
-        const long long b = (long long)blockIdx.x / u.tiles_per_tr;
-        tcu_load(&imap, sm, &bar[0], (int)((long long)blockIdx.x - b * u.tiles_per_tr) * TCU_J, (int)b);
+        long long b;
+        int j0;
+        tcu_tile(u, blockIdx.x, b, j0);
+        tcu_load(&imap, sm, &bar[0], j0, (int)b);
         pending = true;
     }
     for (long long tile = blockIdx.x; tile < u.ntiles; tile += G) {
@@ -357,8 +360,9 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         in_par ^= 1;
         if (t == 0) pending = false;
         long long b;
-        int j;
-        tcu_line(u, tile, t, b, j);
+        int j0;
+        tcu_tile(u, tile, b, j0);
+        const int j = j0 + l;
         // ---- stage 1: row t = points i + 16 m of line l ----
         float2 x[16];
 #pragma unroll
@@ -393,18 +397,23 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         float mx = 0.f;
 #pragma unroll
         for (int m = 0; m < 16; ++m) mx = fmaxf(mx, fmaxf(fabsf(x[m].x), fabsf(x[m].y)));
-#pragma unroll
-        for (int o = 1; o < 16; o <<= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        // (a line's 16 rows are lanes 8 (l & 1) + {0..7, 16..23} of the warp)
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
         const int e1 = (mx >= TCU_LO && mx < TCU_HI) ? 0 : tcu_exp(mx);
+        // the exponent of this thread's stage-2 line (held by lane 8 (l2 & 1) in stage 1)
+        const int e2 = rowk ? __shfl_sync(0xffffffffu, e1, (l2 & 1) << 3) : e1;
         if (e1 == 0) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c]);
+            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c, sbo), &x[4 * c]);
         } else {
             const float s_in = tcu_pow2(-e1);
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] = make_float2(x[m].x * s_in, x[m].y * s_in);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c]);
+            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c, sbo), &x[4 * c]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -413,77 +422,84 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const long long next = tile + G;
             if (next < u.ntiles) {
-                const long long nb = next / u.tiles_per_tr;
-                tcu_load(&imap, sm, &bar[0], (int)(next - nb * u.tiles_per_tr) * TCU_J, (int)nb);
+                long long nb;
+                int nj0;
+                tcu_tile(u, next, nb, nj0);
+                tcu_load(&imap, sm, &bar[0], nj0, (int)nb);
                 pending = true;
             }
-            tcu_mma6(d1, ah, al, bh, bl);
+            tcu_mma6(d1, ah, al, bh, bl, sbo);
             tcu_commit(&bar[1]);
         }
-        bool ok = tcu_wait(&bar[1], mma_par, u.spin);
+        // Each thread's own wait orders its tensor-memory reads and operand
+        // writes after the products; whether every wait succeeded is decided
+        // at the next barrier.  A warp with a wait that gave up touches
+        // nothing (warp-uniform: the tensor-memory loads are .sync.aligned).
+        const bool ok1 = __all_sync(0xffffffffu, tcu_wait(&bar[1], mma_par, u.spin));
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (!__syncthreads_and(ok)) {
+        // ---- stage-1 outputs y[k1] of row t: twiddle, transpose into the stage-2 rows of (l, k1) ----
+        float v[32];
+        if (ok1) {
+            tcu_ld32(d1 + lane_addr, v);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const float2 c = twt[q * 16 + i];
+                const float re = v[2 * q] * c.x - v[2 * q + 1] * c.y;
+                const float im = v[2 * q] * c.y + v[2 * q + 1] * c.x;
+                const int off = tcu_a_off(tcu_row_b(u.out_kind, l, q), i, sbo);
+                const __half2 h = __floats2half2_rn(re, im);
+                const float2 hf = __half22float2(h);
+                *(__half2*)(Ah + off) = h;
+                *(uint32_t*)(Al + off) = tcu_h2(re - hf.x, im - hf.y);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        if (!__syncthreads_and(ok1)) {
             mma_out = true;
             if (t == 0) atomicCAS(&g_tcu_status, 0u, 2u);
             break;
         }
         mma_par ^= 1;
-        // ---- stage-1 outputs y[k1] of row t: twiddle, transpose into stage-2 rows 16 l + k1 ----
-        float v[32];
-        tcu_ld32(d1 + lane_addr, v);
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            tcu_mma6(d2, ah, al, bh, bl, sbo);
+            tcu_commit(&bar[1]);
+        }
+        const bool ok2 = __all_sync(0xffffffffu, tcu_wait(&bar[1], mma_par, u.spin));
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // ---- stage-2 row t (line l2, group k1): outputs k1 + 16 k2, staged in the A region ----
+        unsigned char* ob = Ah;
+        if (ok2) {
+            tcu_ld32(d2 + lane_addr, v);
+            const float g = tcu_pow2(e2) * fscale;
+            const float gi = a.conj_out ? -g : g;
+            if (g != 1.f || gi != 1.f) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const float2 c = twt[q * 16 + i];
-            const float re = v[2 * q] * c.x - v[2 * q + 1] * c.y;
-            const float im = v[2 * q] * c.y + v[2 * q + 1] * c.x;
-            const int off = tcu_a_off(16 * l + q, i);
-            const __half2 h = __floats2half2_rn(re, im);
-            const float2 hf = __half22float2(h);
-            *(__half2*)(Ah + off) = h;
-            *(uint32_t*)(Al + off) = tcu_h2(re - hf.x, im - hf.y);
+                for (int q = 0; q < 16; ++q) {
+                    v[2 * q] *= g;
+                    v[2 * q + 1] *= gi;
+                }
+            }
+            if (rowk) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    *(float2*)(ob + l2 * 2048 + (k2r + 16 * q) * 8) = make_float2(v[2 * q], v[2 * q + 1]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    *(float2*)(ob + tcu_st_off(k2r + 16 * q, l2)) = make_float2(v[2 * q], v[2 * q + 1]);
+            }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (t == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            tcu_mma6(d2, ah, al, bh, bl);
-            tcu_commit(&bar[1]);
-        }
-        ok = tcu_wait(&bar[1], mma_par, u.spin);
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (!__syncthreads_and(ok)) {
+        if (!__syncthreads_and(ok2)) {
             mma_out = true;
             if (t == 0) atomicCAS(&g_tcu_status, 0u, 3u);
             break;
         }
         mma_par ^= 1;
-        // ---- stage-2 row t = 16 l + k1: outputs k1 + 16 k2 of line l, staged in the A region ----
-        tcu_ld32(d2 + lane_addr, v);
-        const float g = tcu_pow2(e1) * fscale;
-        const float gi = a.conj_out ? -g : g;
-        if (g != 1.f || gi != 1.f) {
-#pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                v[2 * q] *= g;
-                v[2 * q + 1] *= gi;
-            }
-        }
-        unsigned char* ob = Ah;
-        if (u.out_kind == TCU_OUT_ROW) {
-#pragma unroll
-            for (int q = 0; q < 16; ++q)
-                *(float2*)(ob + l * 2048 + (i + 16 * q) * 8) = make_float2(v[2 * q], v[2 * q + 1]);
-        } else {
-#pragma unroll
-            for (int q = 0; q < 16; ++q)
-                *(float2*)(ob + tcu_st_off(i + 16 * q, l)) = make_float2(v[2 * q], v[2 * q + 1]);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
         if (t == 0) {
-            const int j0 = (int)(tile - b * u.tiles_per_tr) * TCU_J;
             if (u.out_kind == TCU_OUT_ROW) {
                 asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
                                  (uint64_t)&omap),
@@ -559,15 +575,9 @@ static bool tcu_map(CUtensorMap* m, const void* base, int rank, const cuuint64_t
 
 bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& launched) {
     launched = false;
-    // the shape this kernel covers: lines j of a transform at unit stride,
-    // one batch dimension, plain complex loads and stores, 16-byte aligned
-    if (a.logR != 8 || a.ndims != 2 || a.jpos != 0 || a.in_estride != 1 || a.out_estride != 1) return true;
-    if (a.in_tab || a.out_tab || a.mid || a.vjp || a.logNj < 3 || a.cnt[0] != (1ll << a.logNj)) return true;
-    if (a.logNs_out != 0 && a.logNs_out < 3) return true;
-    if (((uintptr_t)a.in & 15) || ((uintptr_t)a.out & 15) || a.in == a.out) return true;
+    TcuArgs u;
+    if (!tcu_shape(a, u)) return true;
     const long long B = a.cnt[1], Nj = a.cnt[0];
-    if (B < 1 || Nj * B != a.nlines) return true;
-    if (B > 1 && ((a.istr[1] & 1) || (a.ostr[1] & 1) || a.istr[1] <= 0 || a.ostr[1] <= 0)) return true;
     const long long istr = B > 1 ? a.istr[1] * 8 : Nj * 256 * 8;
     const long long ostr = B > 1 ? a.ostr[1] * 8 : Nj * 256 * 8;
     CUtensorMap imap, omap;
@@ -578,21 +588,17 @@ bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& l
         if (!tcu_map(&imap, a.in, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_64B)) return true;
     }
     const int so = a.logNs_out;
-    int kind;
-    if (so == 0) {
-        kind = TCU_OUT_ROW;
+    if (u.out_kind == TCU_OUT_ROW) {
         const cuuint64_t dims[3] = {256, (cuuint64_t)Nj, (cuuint64_t)B};
         const cuuint64_t strides[2] = {2048, (cuuint64_t)ostr};
         const cuuint32_t box[3] = {256, TCU_J, 1};
         if (!tcu_map(&omap, a.out, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_NONE)) return true;
-    } else if (so < a.logNj) {
-        kind = TCU_OUT_COLSPLIT;
+    } else if (u.out_kind == TCU_OUT_COLSPLIT) {
         const cuuint64_t dims[4] = {(cuuint64_t)1 << so, 256, (cuuint64_t)(Nj >> so), (cuuint64_t)B};
         const cuuint64_t strides[3] = {(cuuint64_t)8 << so, (cuuint64_t)8 << (so + 8), (cuuint64_t)ostr};
         const cuuint32_t box[4] = {TCU_J, 256, 1, 1};
         if (!tcu_map(&omap, a.out, 4, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_64B)) return true;
     } else {
-        kind = TCU_OUT_COL;
         const cuuint64_t dims[3] = {(cuuint64_t)Nj, 256, (cuuint64_t)B};
         const cuuint64_t strides[2] = {(cuuint64_t)8 << so, (cuuint64_t)ostr};
         const cuuint32_t box[3] = {TCU_J, 256, 1};
@@ -610,11 +616,6 @@ bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& l
             return false;
         attr = true;
     }
-    TcuArgs u;
-    u.a = a;
-    u.out_kind = kind;
-    u.tiles_per_tr = Nj / TCU_J;
-    u.ntiles = u.tiles_per_tr * B;
     // NOTORIOUS_FFT_TC_UMMA_SPIN / _WITHHOLD: the failure test's short poll limit
     // and a first input copy that is never issued (every CTA's first wait runs out)
     static const long long spin = [] {

@@ -14,10 +14,20 @@
 //    16 l + k1, columns (2i, 2i+1);
 //  * stage 2 rows: z_{l,k1}[k2] = output point k1 + 16 k2 of line l.
 // A operand layout: K-major, no swizzle: 8-row x 16-byte core matrices at
-// row-group stride TCU_SBO and K-chunk stride TCU_LBO (padded so both the
-// row-wise stage-1 writes and the transposed stage-2 writes are free of
-// bank conflicts).  Input tiles arrive by tensor copy with the 64-byte
-// swizzle; outputs leave through the same buffer by tensor store.
+// row-group stride SBO and K-chunk stride TCU_LBO, padded so that the
+// row-wise stage-1 writes and the transposed stage-2 writes are free of bank
+// conflicts.  Input tiles arrive by tensor copy with the 64-byte swizzle;
+// outputs leave through the A region by tensor store.
+//
+// Thread roles.  Stage 1: thread t holds (line l, row i) with the two lines
+// of a warp interleaved in groups of 8 lanes (tcu_role_a), so a half-warp
+// reads 2 lines x 8 rows of the swizzled input tile: 16 distinct bank pairs.
+// Stage 2 (thread t owns row t of the stage-2 operand, line l, output group
+// k1): the same role for column outputs (their staging is the input tile's
+// layout), and l = t / 16, k1 = t mod 16 for row outputs (a half-warp writes
+// 16 consecutive points of one line).  The transposed writes are conflict
+// free with SBO = TCU_SBO_COL (144 mod 32 = 16 banks per row group) for the
+// first and TCU_SBO_ROW (2 x 152 = 16 mod 32) for the second.
 #pragma once
 
 #include "nfft_pass.cuh"
@@ -27,8 +37,9 @@ namespace nfft {
 constexpr int TCU_THREADS = 128;
 constexpr int TCU_J = 8;                       // lines per tile
 constexpr int TCU_MINB = 5;                    // CTAs per SM the kernel is built for
-constexpr int TCU_LBO = 144, TCU_SBO = 672;    // A operand strides (bytes)
-constexpr int TCU_AOP = 16 * TCU_SBO;          // one 128-row operand
+constexpr int TCU_LBO = 144;                   // A operand K-chunk stride (bytes)
+constexpr int TCU_SBO_COL = 576, TCU_SBO_ROW = 608;   // A operand row-group strides by output kind
+constexpr int TCU_AOP = 16 * TCU_SBO_ROW;      // one 128-row operand (either stride)
 constexpr int TCU_BLBO = 128, TCU_BSBO = 512;  // B operand (written once per CTA, unpadded)
 constexpr int TCU_BOP = 4 * TCU_BSBO;          // one 32-row operand
 constexpr int TCU_STAGE = TCU_J * 256 * 8;     // input tile, 64-byte swizzled rows
@@ -39,6 +50,8 @@ constexpr int TCU_OFF_BL = TCU_OFF_BH + TCU_BOP;
 constexpr int TCU_OFF_TW = TCU_OFF_BL + TCU_BOP;   // W_256^{i k1}, stored [k1][i]
 constexpr int TCU_OFF_BAR = TCU_OFF_TW + 256 * 8;  // mbarriers and the tensor-memory address
 constexpr int TCU_SMEM = TCU_OFF_BAR + 64 + 512;   // + alignment of the stage to 512 bytes
+static_assert(2 * TCU_AOP >= TCU_J * 256 * 8, "output staging fits the A region");
+static_assert(16 * TCU_SBO_COL <= TCU_AOP && 4 * TCU_LBO <= TCU_SBO_COL, "A operand strides");
 constexpr int TCU_TCOLS = 64;                      // stage-1 and stage-2 accumulators
 // Range: a radix-16 output is at most 16 sqrt(2) times the largest input
 // component in modulus, so a line whose largest component is below 2^8 keeps
@@ -56,6 +69,7 @@ struct TcuArgs {
     PassArgs a;
     int out_kind;
     long long tiles_per_tr;    // lines per transform / 8
+    int log_tpt;               // log2(tiles_per_tr)
     long long ntiles;
     long long spin;            // poll limit of every wait
     int withhold;              // failure test: the first input copy is never issued
@@ -64,7 +78,7 @@ struct TcuArgs {
 // point (row r, line l) of a 64-byte swizzled tile row (8 lines x 8 bytes)
 NFFT_HD int tcu_st_off(int r, int l) { return r * 64 + (((l >> 1) ^ ((r >> 1) & 3)) << 4) + ((l & 1) << 3); }
 // byte offset of the (re, im) f16 pair kp of A row `row`
-NFFT_HD int tcu_a_off(int row, int kp) { return (row >> 3) * TCU_SBO + (kp >> 2) * TCU_LBO + (row & 7) * 16 + (kp & 3) * 4; }
+NFFT_HD int tcu_a_off(int row, int kp, int sbo) { return (row >> 3) * sbo + (kp >> 2) * TCU_LBO + (row & 7) * 16 + (kp & 3) * 4; }
 NFFT_HD int tcu_b_off(int row, int kp) { return (row >> 3) * TCU_BSBO + (kp >> 2) * TCU_BLBO + (row & 7) * 16 + (kp & 3) * 4; }
 
 // Entry (row n, K column c) of the real form of the radix-16 DFT matrix:
@@ -76,10 +90,66 @@ NFFT_HD float tcu_b_entry(const TwTables<float>* tw, int n, int c) {
     return im ? f.x : f.y;
 }
 
-// Line j of the tile's row t and the pass pre-twiddle exponent k = j mod Ns.
-NFFT_HD void tcu_line(const TcuArgs& u, long long tile, int t, long long& b, int& j) {
-    b = tile / u.tiles_per_tr;
-    j = (int)(tile - b * u.tiles_per_tr) * TCU_J + (t >> 4);
+// Stage-1 role of thread t (line l of the tile, row i) and its inverse.
+NFFT_HD void tcu_role_a(int t, int& l, int& i) {
+    l = ((t >> 5) << 1) | ((t >> 3) & 1);
+    i = (t & 7) | (((t >> 4) & 1) << 3);
+}
+NFFT_HD int tcu_row_a(int l, int i) { return ((l >> 1) << 5) | ((i >> 3) << 4) | ((l & 1) << 3) | (i & 7); }
+// Stage-2 role of thread t (line l, output group k1) and its inverse, by output kind.
+NFFT_HD void tcu_role_b(int kind, int t, int& l, int& k1) {
+    if (kind == TCU_OUT_ROW) {
+        l = t >> 4;
+        k1 = t & 15;
+    } else {
+        tcu_role_a(t, l, k1);
+    }
+}
+NFFT_HD int tcu_row_b(int kind, int l, int k1) { return kind == TCU_OUT_ROW ? 16 * l + k1 : tcu_row_a(l, k1); }
+
+// Transform b and first line j0 of a tile (lines per transform / 8 is a power of two).
+NFFT_HD void tcu_tile(const TcuArgs& u, long long tile, long long& b, int& j0) {
+    b = tile >> u.log_tpt;
+    j0 = (int)(tile & (u.tiles_per_tr - 1)) * TCU_J;
+}
+
+NFFT_HD C2<float> tcu_cmul(C2<float> a, C2<float> b) { return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+// The passes the kernel takes: lines j of a transform at unit stride (one
+// batch dimension), plain complex loads and stores, distinct 16-byte aligned
+// buffers and batch strides, and an output order it can store by tensor map
+// (row out, or column out at Ns >= 8).  Fills the tile counts and the output
+// kind; false (and nothing launched) for any other pass.
+inline bool tcu_shape(const PassArgs& a, TcuArgs& u) {
+    if (a.logR != 8 || a.ndims != 2 || a.jpos != 0 || a.in_estride != 1 || a.out_estride != 1) return false;
+    if (a.in_tab || a.out_tab || a.mid || a.vjp || a.logNj < 3 || a.cnt[0] != (1ll << a.logNj)) return false;
+    if (a.logNs_out != 0 && a.logNs_out < 3) return false;
+    if (((uintptr_t)a.in & 15) || ((uintptr_t)a.out & 15) || a.in == a.out) return false;
+    const long long B = a.cnt[1], Nj = a.cnt[0];
+    if (B < 1 || Nj * B != a.nlines) return false;
+    if (B > 1 && ((a.istr[1] & 1) || (a.ostr[1] & 1) || a.istr[1] <= 0 || a.ostr[1] <= 0)) return false;
+    u.a = a;
+    u.out_kind = a.logNs_out == 0 ? TCU_OUT_ROW : (a.logNs_out < a.logNj ? TCU_OUT_COLSPLIT : TCU_OUT_COL);
+    u.tiles_per_tr = Nj / TCU_J;
+    u.log_tpt = a.logNj - 3;
+    u.ntiles = u.tiles_per_tr * B;
+    u.spin = 1ll << 22;
+    u.withhold = 0;
+    return true;
+}
+
+// Element offsets (complex points) of point r of line j of transform b: the
+// input, and output point p, as the kernel's tensor maps lay them out.
+NFFT_HD long long tcu_in_index(const TcuArgs& u, long long b, int j, int r) {
+    return b * u.a.istr[1] + j + (long long)r * u.a.cnt[0];
+}
+NFFT_HD long long tcu_out_index(const TcuArgs& u, long long b, int j, int p) {
+    const int s = u.a.logNs_out;
+    const long long base = b * u.a.ostr[1];
+    if (u.out_kind == TCU_OUT_ROW) return base + ((long long)j << 8) + p;
+    if (u.out_kind == TCU_OUT_COLSPLIT)
+        return base + ((long long)(j >> s) << (s + 8)) + (j & ((1 << s) - 1)) + ((long long)p << s);
+    return base + j + ((long long)p << s);
 }
 
 // 2^e as a float (e in [-126, 127]; 0 below)
