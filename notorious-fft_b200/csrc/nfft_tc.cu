@@ -232,16 +232,17 @@ __device__ __forceinline__ void tcu_load(const CUtensorMap* map, void* dst, uint
         "l"((uint64_t)map), "r"(c0), "r"(0), "r"(c2), "r"(tcu_smem(bar))
         : "memory");
 }
-// D = Ah Bh + Al Bh + Ah Bl; K = 32 as two steps of 16 (two core matrices each)
-__device__ __forceinline__ void tcu_mma6(uint32_t d, uint32_t ah, uint32_t al, uint32_t bh, uint32_t bl, uint32_t sbo) {
-    // instruction descriptor: FP32 accumulators, FP16 A and B, both K-major, N = 32, M = 128
-    const uint32_t idesc = (1u << 4) | ((uint32_t)(32 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+// D = Ah Bh + Al Bh + Ah Bl; K = 32 as two steps of 16 (two K chunks / K-row groups each)
+__device__ __forceinline__ void tcu_mma6(uint32_t d, uint32_t ah, uint32_t al, uint32_t bh, uint32_t bl, bool a_mmajor) {
+    // instruction descriptor: FP32 accumulators, FP16 A and B, B K-major, A K- or M-major, N = 32, M = 128
+    const uint32_t idesc = (1u << 4) | (a_mmajor ? (1u << 15) : 0u) | ((uint32_t)(32 >> 3) << 17) |
+                           ((uint32_t)(128 >> 4) << 24);
     const uint32_t as[3] = {ah, al, ah}, bs[3] = {bh, bh, bl};
 #pragma unroll
     for (int q = 0; q < 3; ++q)
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
-            const uint64_t ad = tcu_desc(as[q] + ks * 2 * TCU_LBO, TCU_LBO, sbo);
+            const uint64_t ad = tcu_desc(as[q] + ks * 2 * TCU_LBO, TCU_LBO, TCU_SBO);
             const uint64_t bd = tcu_desc(bs[q] + ks * 2 * TCU_BLBO, TCU_BLBO, TCU_BSBO);
             const uint32_t acc = (q | ks) ? 1u : 0u;
             asm volatile(
@@ -299,7 +300,6 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     tcu_role_a(t, l, i);
     tcu_role_b(u.out_kind, t, l2, k2r);
     const bool rowk = u.out_kind == TCU_OUT_ROW;
-    const int sbo = rowk ? TCU_SBO_ROW : TCU_SBO_COL;
     const long long G = gridDim.x;
     unsigned char* Ah = sm + TCU_OFF_AH;
     unsigned char* Al = sm + TCU_OFF_AL;
@@ -407,13 +407,13 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         const int e2 = rowk ? __shfl_sync(0xffffffffu, e1, (l2 & 1) << 3) : e1;
         if (e1 == 0) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c, sbo), &x[4 * c]);
+            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c]);
         } else {
             const float s_in = tcu_pow2(-e1);
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] = make_float2(x[m].x * s_in, x[m].y * s_in);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c, sbo), &x[4 * c]);
+            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
                 tcu_load(&imap, sm, &bar[0], nj0, (int)nb);
                 pending = true;
             }
-            tcu_mma6(d1, ah, al, bh, bl, sbo);
+            tcu_mma6(d1, ah, al, bh, bl, false);
             tcu_commit(&bar[1]);
         }
         // Each thread's own wait orders its tensor-memory reads and operand
@@ -437,7 +437,8 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         // nothing (warp-uniform: the tensor-memory loads are .sync.aligned).
         const bool ok1 = __all_sync(0xffffffffu, tcu_wait(&bar[1], mma_par, u.spin));
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // ---- stage-1 outputs y[k1] of row t: twiddle, transpose into the stage-2 rows of (l, k1) ----
+        // ---- stage-1 outputs y[k1] of row t: twiddle; column (2i, 2i+1) of the
+        //      M-major stage-2 rows of (l, k1), 8 k1 per 16-byte unit ----
         float v[32];
         if (ok1) {
             tcu_ld32(d1 + lane_addr, v);
@@ -446,11 +447,26 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
                 const float2 c = twt[q * 16 + i];
                 const float re = v[2 * q] * c.x - v[2 * q + 1] * c.y;
                 const float im = v[2 * q] * c.y + v[2 * q + 1] * c.x;
-                const int off = tcu_a_off(tcu_row_b(u.out_kind, l, q), i, sbo);
-                const __half2 h = __floats2half2_rn(re, im);
-                const float2 hf = __half22float2(h);
-                *(__half2*)(Ah + off) = h;
-                *(uint32_t*)(Al + off) = tcu_h2(re - hf.x, im - hf.y);
+                v[2 * q] = re;
+                v[2 * q + 1] = im;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int off = tcu_at_off(tcu_row_b(u.out_kind, l, 8 * h), 2 * i);
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    uint32_t hh[4], ll[4];
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) {
+                        const float x0 = v[2 * (8 * h + 2 * p) + c], x1 = v[2 * (8 * h + 2 * p + 1) + c];
+                        const __half2 hv = __floats2half2_rn(x0, x1);
+                        const float2 hf = __half22float2(hv);
+                        hh[p] = *(const uint32_t*)&hv;
+                        ll[p] = tcu_h2(x0 - hf.x, x1 - hf.y);
+                    }
+                    *(uint4*)(Ah + off + 16 * c) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+                    *(uint4*)(Al + off + 16 * c) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+                }
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -463,7 +479,7 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         mma_par ^= 1;
         if (t == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            tcu_mma6(d2, ah, al, bh, bl, sbo);
+            tcu_mma6(d2, ah, al, bh, bl, true);
             tcu_commit(&bar[1]);
         }
         const bool ok2 = __all_sync(0xffffffffu, tcu_wait(&bar[1], mma_par, u.spin));
@@ -577,9 +593,9 @@ bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& l
     launched = false;
     TcuArgs u;
     if (!tcu_shape(a, u)) return true;
-    const long long B = a.cnt[1], Nj = a.cnt[0];
-    const long long istr = B > 1 ? a.istr[1] * 8 : Nj * 256 * 8;
-    const long long ostr = B > 1 ? a.ostr[1] * 8 : Nj * 256 * 8;
+    const long long B = u.a.cnt[1], Nj = u.a.cnt[0];
+    const long long istr = B > 1 ? u.a.istr[1] * 8 : Nj * 256 * 8;
+    const long long ostr = B > 1 ? u.a.ostr[1] * 8 : Nj * 256 * 8;
     CUtensorMap imap, omap;
     {
         const cuuint64_t dims[3] = {(cuuint64_t)Nj, 256, (cuuint64_t)B};

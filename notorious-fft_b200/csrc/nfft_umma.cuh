@@ -10,14 +10,20 @@
 //    (pass pre-twiddled, scaled by a power of two when out of range), columns
 //    (2m, 2m+1) = (re, im); B is the real form of the radix-16 DFT matrix;
 //    D row t = y_{l,i}[k1];
-//  * the internal twiddles W_256^{i k1}, transposed into stage-2 rows
-//    16 l + k1, columns (2i, 2i+1);
+//  * the internal twiddles W_256^{i k1}; stage 2 row (l, k1) column
+//    (2i, 2i+1) is the twiddled y_{l,i}[k1], so the stage-2 operand is the
+//    stage-1 result transposed per line: it is written M-major (8 rows of
+//    one column per 16 bytes), which is a plain row of the thread that holds
+//    y_{l,i}, and the product reads it with the A-transpose bit;
 //  * stage 2 rows: z_{l,k1}[k2] = output point k1 + 16 k2 of line l.
-// A operand layout: K-major, no swizzle: 8-row x 16-byte core matrices at
-// row-group stride SBO and K-chunk stride TCU_LBO, padded so that the
-// row-wise stage-1 writes and the transposed stage-2 writes are free of bank
-// conflicts.  Input tiles arrive by tensor copy with the 64-byte swizzle;
-// outputs leave through the A region by tensor store.
+// A operand layouts, no swizzle, the same two strides:
+//  * stage 1, K-major: rows of 8 x 16-byte core matrices, K chunks (8 f16)
+//    at TCU_LBO, 8-row groups at TCU_SBO;
+//  * stage 2, M-major: 16-byte rows of 8 M values, K rows 16 bytes apart,
+//    groups of 8 K rows at TCU_LBO, groups of 8 M at TCU_SBO.
+// The 16-byte units of 8 consecutive lanes land in 8 distinct bank groups
+// (TCU_LBO / 16 is odd).  Input tiles arrive by tensor copy with the 64-byte
+// swizzle; outputs leave through the A region by tensor store.
 //
 // Thread roles.  Stage 1: thread t holds (line l, row i) with the two lines
 // of a warp interleaved in groups of 8 lanes (tcu_role_a), so a half-warp
@@ -25,9 +31,7 @@
 // Stage 2 (thread t owns row t of the stage-2 operand, line l, output group
 // k1): the same role for column outputs (their staging is the input tile's
 // layout), and l = t / 16, k1 = t mod 16 for row outputs (a half-warp writes
-// 16 consecutive points of one line).  The transposed writes are conflict
-// free with SBO = TCU_SBO_COL (144 mod 32 = 16 banks per row group) for the
-// first and TCU_SBO_ROW (2 x 152 = 16 mod 32) for the second.
+// 16 consecutive points of one line).
 #pragma once
 
 #include "nfft_pass.cuh"
@@ -37,9 +41,8 @@ namespace nfft {
 constexpr int TCU_THREADS = 128;
 constexpr int TCU_J = 8;                       // lines per tile
 constexpr int TCU_MINB = 5;                    // CTAs per SM the kernel is built for
-constexpr int TCU_LBO = 144;                   // A operand K-chunk stride (bytes)
-constexpr int TCU_SBO_COL = 576, TCU_SBO_ROW = 608;   // A operand row-group strides by output kind
-constexpr int TCU_AOP = 16 * TCU_SBO_ROW;      // one 128-row operand (either stride)
+constexpr int TCU_LBO = 144, TCU_SBO = 576;    // A operand strides (bytes)
+constexpr int TCU_AOP = 16 * TCU_SBO;          // one 128-row operand
 constexpr int TCU_BLBO = 128, TCU_BSBO = 512;  // B operand (written once per CTA, unpadded)
 constexpr int TCU_BOP = 4 * TCU_BSBO;          // one 32-row operand
 constexpr int TCU_STAGE = TCU_J * 256 * 8;     // input tile, 64-byte swizzled rows
@@ -51,7 +54,7 @@ constexpr int TCU_OFF_TW = TCU_OFF_BL + TCU_BOP;   // W_256^{i k1}, stored [k1][
 constexpr int TCU_OFF_BAR = TCU_OFF_TW + 256 * 8;  // mbarriers and the tensor-memory address
 constexpr int TCU_SMEM = TCU_OFF_BAR + 64 + 512;   // + alignment of the stage to 512 bytes
 static_assert(2 * TCU_AOP >= TCU_J * 256 * 8, "output staging fits the A region");
-static_assert(16 * TCU_SBO_COL <= TCU_AOP && 4 * TCU_LBO <= TCU_SBO_COL, "A operand strides");
+static_assert(4 * TCU_LBO <= TCU_SBO && ((TCU_LBO / 16) & 1), "A operand strides");
 constexpr int TCU_TCOLS = 64;                      // stage-1 and stage-2 accumulators
 // Range: a radix-16 output is at most 16 sqrt(2) times the largest input
 // component in modulus, so a line whose largest component is below 2^8 keeps
@@ -77,8 +80,10 @@ struct TcuArgs {
 
 // point (row r, line l) of a 64-byte swizzled tile row (8 lines x 8 bytes)
 NFFT_HD int tcu_st_off(int r, int l) { return r * 64 + (((l >> 1) ^ ((r >> 1) & 3)) << 4) + ((l & 1) << 3); }
-// byte offset of the (re, im) f16 pair kp of A row `row`
-NFFT_HD int tcu_a_off(int row, int kp, int sbo) { return (row >> 3) * sbo + (kp >> 2) * TCU_LBO + (row & 7) * 16 + (kp & 3) * 4; }
+// byte offset of the (re, im) f16 pair kp of K-major A row `row`
+NFFT_HD int tcu_a_off(int row, int kp) { return (row >> 3) * TCU_SBO + (kp >> 2) * TCU_LBO + (row & 7) * 16 + (kp & 3) * 4; }
+// byte offset of the 16-byte unit (rows m0 .. m0 + 7, column k) of M-major A (m0 a multiple of 8)
+NFFT_HD int tcu_at_off(int m0, int k) { return (m0 >> 3) * TCU_SBO + (k >> 3) * TCU_LBO + (k & 7) * 16; }
 NFFT_HD int tcu_b_off(int row, int kp) { return (row >> 3) * TCU_BSBO + (kp >> 2) * TCU_BLBO + (row & 7) * 16 + (kp & 3) * 4; }
 
 // Entry (row n, K column c) of the real form of the radix-16 DFT matrix:
@@ -116,19 +121,26 @@ NFFT_HD void tcu_tile(const TcuArgs& u, long long tile, long long& b, int& j0) {
 NFFT_HD C2<float> tcu_cmul(C2<float> a, C2<float> b) { return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 
 // The passes the kernel takes: lines j of a transform at unit stride (one
-// batch dimension), plain complex loads and stores, distinct 16-byte aligned
-// buffers and batch strides, and an output order it can store by tensor map
-// (row out, or column out at Ns >= 8).  Fills the tile counts and the output
-// kind; false (and nothing launched) for any other pass.
+// transform, or a batch dimension outside j), plain complex loads and stores,
+// distinct 16-byte aligned buffers and batch strides, and an output order it
+// can store by tensor map (row out, or column out at Ns >= 8).  Fills the
+// tile counts and the output kind; false (and nothing launched) for any
+// other pass.
 inline bool tcu_shape(const PassArgs& a, TcuArgs& u) {
-    if (a.logR != 8 || a.ndims != 2 || a.jpos != 0 || a.in_estride != 1 || a.out_estride != 1) return false;
+    if (a.logR != 8 || (a.ndims != 1 && a.ndims != 2) || a.jpos != 0) return false;
+    if (a.in_estride != 1 || a.out_estride != 1) return false;
     if (a.in_tab || a.out_tab || a.mid || a.vjp || a.logNj < 3 || a.cnt[0] != (1ll << a.logNj)) return false;
     if (a.logNs_out != 0 && a.logNs_out < 3) return false;
     if (((uintptr_t)a.in & 15) || ((uintptr_t)a.out & 15) || a.in == a.out) return false;
-    const long long B = a.cnt[1], Nj = a.cnt[0];
+    const long long B = a.ndims == 2 ? a.cnt[1] : 1, Nj = a.cnt[0];
     if (B < 1 || Nj * B != a.nlines) return false;
     if (B > 1 && ((a.istr[1] & 1) || (a.ostr[1] & 1) || a.istr[1] <= 0 || a.ostr[1] <= 0)) return false;
     u.a = a;
+    if (a.ndims == 1) {   // one transform: batch stride unused, count 1
+        u.a.ndims = 2;
+        u.a.cnt[1] = 1;
+        u.a.istr[1] = u.a.ostr[1] = 0;
+    }
     u.out_kind = a.logNs_out == 0 ? TCU_OUT_ROW : (a.logNs_out < a.logNj ? TCU_OUT_COLSPLIT : TCU_OUT_COL);
     u.tiles_per_tr = Nj / TCU_J;
     u.log_tpt = a.logNj - 3;

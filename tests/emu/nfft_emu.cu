@@ -199,6 +199,7 @@ __host__ __device__ void nfft_emu_smem_check(int idx) {
 #include "../../notorious-fft_b200/csrc/nfft_lean_list.h"
 #include "../../notorious-fft_b200/csrc/nfft_tc.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_tc_lean.cuh"
+#include "../../notorious-fft_b200/csrc/nfft_umma.cuh"
 #include "../../notorious-fft_b200/csrc/nfft_queue.h"
 
 // ---------------------------------------------------------------------------
@@ -627,14 +628,181 @@ static void emu_tcl_stage(const TcA* A, uint32_t (*xb)[2][2][2][2], float (*acc)
         }
 }
 
-// The tcgen05 radix-256 pass has no CPU model here: emulated runs take the
-// warp-level kernel's path for every radix-256 pass of the split form.
-bool tc_umma_enabled() { return false; }
-bool try_launch_tc_umma(const PassArgs&, int, cudaStream_t, bool& launched) {
-    launched = false;
-    return true;
+// ---- radix-256 split tensor-core pass on tcgen05 (nfft_tc.cu, layout and
+// index maps in nfft_umma.cuh): the kernel's phases for the 128 threads of a
+// tile, in order, around host models of what the hardware does between them:
+//  * the tensor copy in: box (8 lines x 256 rows) written row-major and
+//    64-byte swizzled by address bits (bits 4-5 ^= bits 7-8);
+//  * the products: D = Ah Bh + Al Bh + Ah Bl with every operand element read
+//    through the descriptors' strides (stage 1 A and B K-major, stage 2 A
+//    M-major), FP16 values, sums in double, rounded to float;
+//  * tensor memory: D row t is thread t's;
+//  * the tensor store out: the same box layouts read back.
+static long long g_umma_launches = 0, g_umma_kind[3] = {0, 0, 0};
+bool tc_umma_enabled() {
+    const char* e = getenv("NOTORIOUS_FFT_TC_UMMA");
+    return !e || atoi(e) != 0;
 }
 unsigned tc_umma_take_status() { return 0; }
+
+static int emu_swz64(int o) { return o ^ (((o >> 7) & 3) << 4); }
+static float emu_f16(const unsigned char* base, int off) {
+    __half h;
+    memcpy(&h, base + off, 2);
+    return __half2float(h);
+}
+// D[m][n] = sum over the three hi / lo products, K = 32 (element offsets per the descriptors)
+static void emu_umma(const unsigned char* ah, const unsigned char* al, const unsigned char* bh,
+                     const unsigned char* bl, bool a_mmajor, float (*d)[32]) {
+    auto aoff = [&](int m, int k) {
+        return a_mmajor ? (m >> 3) * TCU_SBO + (k >> 3) * TCU_LBO + (k & 7) * 16 + (m & 7) * 2
+                        : (m >> 3) * TCU_SBO + (k >> 3) * TCU_LBO + (m & 7) * 16 + (k & 7) * 2;
+    };
+    auto boff = [](int n, int k) { return (n >> 3) * TCU_BSBO + (k >> 3) * TCU_BLBO + (n & 7) * 16 + (k & 7) * 2; };
+    for (int m = 0; m < 128; ++m)
+        for (int n = 0; n < 32; ++n) {
+            double acc = 0;
+            for (int k = 0; k < 32; ++k) {
+                const double xh = emu_f16(ah, aoff(m, k)), xl = emu_f16(al, aoff(m, k));
+                const double fh = emu_f16(bh, boff(n, k)), fl = emu_f16(bl, boff(n, k));
+                acc += xh * fh + xl * fh + xh * fl;
+            }
+            d[m][n] = (float)acc;
+        }
+}
+
+bool try_launch_tc_umma(const PassArgs& a, int, cudaStream_t, bool& launched) {
+    launched = false;
+    if (sizeof(real_t) != 4 || !tc_umma_enabled()) return true;
+    TcuArgs u;
+    if (!tcu_shape(a, u)) return true;
+    launched = true;
+    g_launches++;
+    g_umma_launches++;
+    g_umma_kind[u.out_kind]++;
+    const TwTables<float>* tw = (const TwTables<float>*)a.tw;
+    // constants: the DFT matrix operands, the internal twiddles [k1][i]
+    std::vector<unsigned char> Bh(TCU_BOP), Bl(TCU_BOP);
+    for (int n = 0; n < 32; ++n)
+        for (int c = 0; c < 32; ++c) {
+            const float v = tcu_b_entry(tw, n, c);
+            const __half h = __float2half_rn(v), lo = __float2half_rn(v - __half2float(h));
+            const int off = tcu_b_off(n, c >> 1) + (c & 1) * 2;
+            memcpy(&Bh[off], &h, 2);
+            memcpy(&Bl[off], &lo, 2);
+        }
+    float2 twt[256];
+    for (int q = 0; q < 256; ++q) {
+        const int ii = q >> 4, k1 = q & 15;
+        const C2<float> c = NFFT_GLD(&tw->t[0][(ii * k1 * 16) & (TW_SIZE - 1)]);
+        twt[k1 * 16 + ii] = make_float2(c.x, c.y);
+    }
+    std::vector<unsigned char> stage(TCU_STAGE), A(2 * TCU_AOP);
+    unsigned char* Ah = A.data();
+    unsigned char* Al = A.data() + TCU_AOP;
+    static float D1[128][32], D2[128][32];
+    const float2* in = (const float2*)u.a.in;
+    float2* out = (float2*)u.a.out;
+    const float fscale = (float)a.scale;
+    for (long long tile = 0; tile < u.ntiles; ++tile) {
+        long long b;
+        int j0;
+        tcu_tile(u, tile, b, j0);
+        for (auto& x : stage) x = 0xff;   // NaN bytes: a read of an unwritten slot shows
+        for (auto& x : A) x = 0xff;
+        for (int l = 0; l < TCU_J; ++l)
+            for (int r = 0; r < 256; ++r) {
+                const float2 v = NFFT_GLD(in + tcu_in_index(u, b, j0 + l, r));
+                memcpy(&stage[emu_swz64((r * TCU_J + l) * 8)], &v, 8);
+            }
+        // stage 1: rows, pre-twiddles, per-line exponent, split
+        static float2 X[128][16];
+        float mx[TCU_J] = {0};
+        int e1[TCU_J];
+        for (int t = 0; t < 128; ++t) {
+            int l, i;
+            tcu_role_a(t, l, i);
+            const int j = j0 + l;
+            float2* x = X[t];
+            for (int m = 0; m < 16; ++m) memcpy(&x[m], &stage[tcu_st_off(i + 16 * m, l)], 8);
+            if (a.conj_in)
+                for (int m = 0; m < 16; ++m) x[m].y = -x[m].y;
+            const long long k = a.logNs > 0 ? (j & ((1ll << a.logNs) - 1)) : 0;
+            if (k) {
+                const C2<float> wb = twiddle<float>(tw, (uint64_t)i * (uint64_t)k, a.logNs + 8);
+                const C2<float> s1 = twiddle<float>(tw, (uint64_t)k, a.logNs + 4);
+                C2<float> pw[16];
+                pw[0] = wb;
+                pw[1] = tcu_cmul(wb, s1);
+                const C2<float> s2 = tcu_cmul(s1, s1), s4 = tcu_cmul(s2, s2), s8 = tcu_cmul(s4, s4);
+                pw[2] = tcu_cmul(wb, s2);
+                pw[3] = tcu_cmul(pw[1], s2);
+                for (int m = 4; m < 8; ++m) pw[m] = tcu_cmul(pw[m - 4], s4);
+                for (int m = 8; m < 16; ++m) pw[m] = tcu_cmul(pw[m - 8], s8);
+                for (int m = 0; m < 16; ++m) x[m] = tcu_cmul(x[m], pw[m]);
+            }
+            for (int m = 0; m < 16; ++m) mx[l] = fmaxf(mx[l], fmaxf(fabsf(x[m].x), fabsf(x[m].y)));
+        }
+        for (int l = 0; l < TCU_J; ++l) e1[l] = (mx[l] >= TCU_LO && mx[l] < TCU_HI) ? 0 : tcu_exp(mx[l]);
+        for (int t = 0; t < 128; ++t) {
+            int l, i;
+            tcu_role_a(t, l, i);
+            const float s_in = tcu_pow2(-e1[l]);
+            for (int m = 0; m < 16; ++m) {
+                const float re = X[t][m].x * s_in, im = X[t][m].y * s_in;
+                const __half hr = __float2half_rn(re), hi = __float2half_rn(im);
+                const __half lr = __float2half_rn(re - __half2float(hr)), li = __float2half_rn(im - __half2float(hi));
+                const int off = tcu_a_off(t, m);
+                memcpy(Ah + off, &hr, 2);
+                memcpy(Ah + off + 2, &hi, 2);
+                memcpy(Al + off, &lr, 2);
+                memcpy(Al + off + 2, &li, 2);
+            }
+        }
+        emu_umma(Ah, Al, Bh.data(), Bl.data(), false, D1);
+        // stage-1 outputs: twiddle, M-major stage-2 operand
+        for (auto& x : A) x = 0xff;
+        for (int t = 0; t < 128; ++t) {
+            int l, i;
+            tcu_role_a(t, l, i);
+            for (int q = 0; q < 16; ++q) {
+                const float2 c = twt[q * 16 + i];
+                const float re = D1[t][2 * q] * c.x - D1[t][2 * q + 1] * c.y;
+                const float im = D1[t][2 * q] * c.y + D1[t][2 * q + 1] * c.x;
+                const int off = tcu_at_off(tcu_row_b(u.out_kind, l, q & ~7), 2 * i) + (q & 7) * 2;
+                const float pr[2] = {re, im};
+                for (int c2 = 0; c2 < 2; ++c2) {
+                    const __half h = __float2half_rn(pr[c2]);
+                    const __half lo = __float2half_rn(pr[c2] - __half2float(h));
+                    memcpy(Ah + off + 16 * c2, &h, 2);
+                    memcpy(Al + off + 16 * c2, &lo, 2);
+                }
+            }
+        }
+        emu_umma(Ah, Al, Bh.data(), Bl.data(), true, D2);
+        // stage 2: scale, stage in the A region, tensor store
+        for (auto& x : A) x = 0xff;
+        for (int t = 0; t < 128; ++t) {
+            int l2, k1;
+            tcu_role_b(u.out_kind, t, l2, k1);
+            const float g = tcu_pow2(e1[l2]) * fscale;
+            const float gi = a.conj_out ? -g : g;
+            for (int q = 0; q < 16; ++q) {
+                const float2 v = make_float2(D2[t][2 * q] * g, D2[t][2 * q + 1] * gi);
+                const int off = u.out_kind == TCU_OUT_ROW ? l2 * 2048 + (k1 + 16 * q) * 8 : tcu_st_off(k1 + 16 * q, l2);
+                memcpy(Ah + off, &v, 8);
+            }
+        }
+        for (int l = 0; l < TCU_J; ++l)
+            for (int p = 0; p < 256; ++p) {
+                const int lin = u.out_kind == TCU_OUT_ROW ? (l * 256 + p) * 8 : emu_swz64((p * TCU_J + l) * 8);
+                float2 v;
+                memcpy(&v, Ah + lin, 8);
+                NFFT_GST(out + tcu_out_index(u, b, j0 + l, p), v);
+            }
+    }
+    return true;
+}
 
 bool tc_lean_enabled() {
     const char* e = getenv("NOTORIOUS_FFT_TC_LEAN");
@@ -829,4 +997,6 @@ long long nfft_emu_launches(void) { return nfft::g_launches; }
 long long nfft_emu_lean_launches(void) { return nfft::g_lean_launches; }
 long long nfft_emu_checks(void) { return emu::n_checks; }
 long long nfft_emu_queue_items(void) { return nfft::g_queue_items; }
+long long nfft_emu_umma_launches(void) { return nfft::g_umma_launches; }
+long long nfft_emu_umma_kind_launches(int k) { return (k >= 0 && k < 3) ? nfft::g_umma_kind[k] : -1; }
 }

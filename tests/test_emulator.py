@@ -9,8 +9,12 @@ API, and the adjoints against the transposed transforms and finite
 differences.  Tolerances are the north-star ones (1e-13 log2 N for double,
 1e-6 log2 N for float).
 """
+import ctypes
+import json
 import math
 import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -18,6 +22,7 @@ import scipy.fft as sf
 
 from oracle import rel_l2
 
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 R2R = ["dct2", "dst2", "dct3", "dst3", "dct4", "dst4"]
 
 
@@ -306,6 +311,95 @@ print(float(np.linalg.norm(y - ref) / np.linalg.norm(ref)))
     assert float(r.stdout.strip().splitlines()[-1]) < 1e-13 * 17
 
 
+@pytest.mark.parametrize("n,batch,pad,kinds", [(1 << 16, 3, 0, [1, 0, 1]), (1 << 16, 2, 2, [1, 0, 1]),
+                                               (1 << 16, 1, 0, [1, 0, 1]), (1 << 17, 2, 0, [0, 0, 1])])
+def test_emu_split_tc_tcgen05_model(emu_f, oracle_d, n, batch, pad, kinds, monkeypatch):
+    """The tcgen05 radix-256 pass through its CPU model (tensor copy with the
+    64-byte swizzle, operands read through the descriptor strides: stage 1
+    K-major, stage 2 M-major; tensor stores): the row-out first pass and the
+    column-out last pass of 2^16 (batches of 3, 2 with a batch stride of
+    n + 2 points, and 1), the column-out radix-256 pass of 2^17 (512 x 256);
+    one transform scaled by 1e4 and one by 1e-4 (per-line power-of-two
+    scaling), forward and inverse, every transform within the split form's
+    bar of the FP64 oracle and the model launched for the expected output
+    kinds (row, column split at Ns, column)."""
+    from notorious_fft import FORM_SPLIT_TC
+    monkeypatch.setenv("NOTORIOUS_FFT_TC_UMMA", "1")
+    count = emu_f.lib.nfft_emu_umma_kind_launches
+    count.restype = ctypes.c_longlong
+    count.argtypes = [ctypes.c_int]
+    rng = np.random.default_rng(n + batch + pad)
+    x = rng.standard_normal((batch, n)) + 1j * rng.standard_normal((batch, n))
+    x[0] *= 1e4
+    x[-1] *= 1e-4
+    x = x.astype(np.complex64)
+    dist = n + pad
+    xb = np.zeros(batch * dist, np.complex64)
+    for b in range(batch):
+        xb[b * dist:b * dist + n] = x[b]
+    bar = max(2e-6, 1e-6 * ((n.bit_length() - 1 + 7) // 8))
+    with emu_f.mkaux("dft", [n]) as a:
+        a.set_form(FORM_SPLIT_TC)
+        for kind in ("dft", "invdft"):
+            before = [count(k) for k in range(3)]
+            yb = np.zeros(batch * dist, np.complex64)
+            a.batched(kind, xb, yb, batch, dist, dist)
+            assert [count(k) - before[k] for k in range(3)] == kinds
+            ref = oracle_d.transform(kind, x.astype(np.complex128))
+            errs = [rel_l2(yb[b * dist:b * dist + n], ref[b]) for b in range(batch)]
+            assert max(errs) <= bar, (kind, errs)
+
+
+UMMA_SPLIT_CHILD = r"""
+import ctypes, json, sys, numpy as np
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[2])
+from notorious_fft import Library, FORM_SPLIT_TC
+from oracle import Oracle, rel_l2
+L = Library(sys.argv[3])
+kinds = L.lib.nfft_emu_umma_kind_launches
+kinds.restype = ctypes.c_longlong
+kinds.argtypes = [ctypes.c_int]
+n, B = 1 << 15, 2
+rng = np.random.default_rng(15)
+x = (rng.standard_normal((B, n)) + 1j * rng.standard_normal((B, n))).astype(np.complex64)
+x[1] *= 300.0
+out = {}
+with L.mkaux("dft", [n]) as a:
+    a.set_form(FORM_SPLIT_TC)
+    out["split"] = a.schedule()[0]
+    for kind in ("dft", "invdft"):
+        k0 = [kinds(k) for k in range(3)]
+        y = np.zeros_like(x)
+        a.batched(kind, x, y, B, n, n)
+        ref = Oracle().transform(kind, x.astype(np.complex128))
+        out[kind] = {"kinds": [kinds(k) - k0[k] for k in range(3)],
+                     "err": max(rel_l2(y[b], ref[b]) for b in range(B))}
+print(json.dumps(out))
+"""
+
+
+def test_emu_split_tc_tcgen05_model_column_split(tmp_path):
+    """The column-out pass with the line index split at Ns (a radix-256 pass
+    in the middle of a transform: 2^15 as 8 x 256 x 16 through a tune-cache
+    split; Ns = 8 < 128 lines) through the tcgen05 model, forward and inverse,
+    one transform scaled by 300 (lines above the unscaled range)."""
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "tests", "emu")], check=True)
+    cache = tmp_path / "tune.json"
+    entry = {"device": "emulated sm_100 sm_100 driver 0", "key": "f32:plan:dft:32768", "split": [3, 8, 4],
+             "logt": 0, "us": 1.0}
+    cache.write_text('{"format": "notorious_fft tune cache 1", "entries": [\n' + json.dumps(entry) + "\n]}\n")
+    env = dict(os.environ, NOTORIOUS_FFT_TUNE_CACHE=str(cache), NOTORIOUS_FFT_TC_UMMA="1")
+    r = subprocess.run([sys.executable, "-c", UMMA_SPLIT_CHILD, os.path.join(ROOT, "notorious-fft_b200"),
+                        os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests", "emu", "_build", "libnfft_emu_f.so")],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    assert res["split"] == [3, 8, 4]
+    for kind in ("dft", "invdft"):
+        assert res[kind]["kinds"] == [0, 1, 0], res
+        assert res[kind]["err"] <= 3e-6, res
+
+
 @pytest.mark.parametrize("n,batch", [(256, 5), (1 << 16, 3), (4096, 3)])
 @pytest.mark.parametrize("tc_lean", ["1", "0"])
 def test_emu_split_tc_form(emu_f, oracle_d, n, batch, tc_lean, monkeypatch):
@@ -317,6 +411,7 @@ def test_emu_split_tc_form(emu_f, oracle_d, n, batch, tc_lean, monkeypatch):
     FP64 oracle."""
     from notorious_fft import FORM_SPLIT_TC
     monkeypatch.setenv("NOTORIOUS_FFT_TC_LEAN", tc_lean)
+    monkeypatch.setenv("NOTORIOUS_FFT_TC_UMMA", "0")
     rng = np.random.default_rng(n + batch)
     x = rng.standard_normal((batch, n)) + 1j * rng.standard_normal((batch, n))
     x[0] *= 1e4
