@@ -182,9 +182,10 @@ bool launch_tc_lean(const PassArgs& a, int sm_count, cudaStream_t s) {
 
 // ---------------------------------------------------------------------------
 // Radix-256 passes on tcgen05 (layout: nfft_umma.cuh).  Persistent CTAs of
-// 128 threads, one tile (8 lines) at a time; the next tile's input copy runs
-// while the current one is transformed; thread t owns stage-1 row t and
-// stage-2 row t (line t >> 4), one thread issues the products.  Every wait
+// TCU_TEAMS teams of 128 threads; a team transforms one tile (8 lines) at a
+// time, the next tile's input copy running while the current one is
+// transformed; thread t of a team owns stage-1 row t and stage-2 row t, one
+// thread of the team issues its products.  Every wait
 // polls at most TcuArgs::spin times and at most 2 s; a wait that gives up
 // records its kind (1: input copy, 2 / 3: stage-1 / stage-2 products) in
 // g_tcu_status, lets the copies and products in flight finish (bounded),
@@ -268,6 +269,28 @@ __device__ __forceinline__ void tcu_ld32(uint32_t taddr, float* v) {
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+// named barrier of team 0 (id 1) or team 1 (id 2) over its 128 threads, plain
+// and with an AND vote (immediate ids: the kernel reserves three barriers)
+__device__ __forceinline__ void tcu_team_sync(int team) {
+    if (team) asm volatile("bar.sync 2, 128;" ::: "memory");
+    else asm volatile("bar.sync 1, 128;" ::: "memory");
+}
+__device__ __forceinline__ bool tcu_team_and(int team, bool p) {
+    unsigned r;
+    if (team)
+        asm volatile("{\n .reg .pred q, o;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred o, 2, 128, q;\n"
+                     " selp.u32 %0, 1, 0, o;\n}"
+                     : "=r"(r)
+                     : "r"((unsigned)p)
+                     : "memory");
+    else
+        asm volatile("{\n .reg .pred q, o;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred o, 1, 128, q;\n"
+                     " selp.u32 %0, 1, 0, o;\n}"
+                     : "=r"(r)
+                     : "r"((unsigned)p)
+                     : "memory");
+    return r != 0;
+}
 __device__ __forceinline__ uint32_t tcu_h2(float re, float im) {
     const __half2 h = __floats2half2_rn(re, im);
     return *(const uint32_t*)&h;
@@ -291,18 +314,20 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     tc_umma_kernel(const TcuArgs u, const __grid_constant__ CUtensorMap imap, const __grid_constant__ CUtensorMap omap) {
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char* sm = smraw + ((512 - (tcu_smem(smraw) & 511)) & 511);
-    uint64_t* bar = (uint64_t*)(sm + TCU_OFF_BAR);   // [0] input tile, [1] products
-    uint32_t* tslot = (uint32_t*)(sm + TCU_OFF_BAR + 16);
+    const int t = threadIdx.x, team = t >> 7, tt = t & 127, w = tt >> 5;
+    unsigned char* stg = sm + team * TCU_TEAM_BYTES;       // the team's input stage
+    uint64_t* bar = (uint64_t*)(sm + TCU_OFF_BAR) + 2 * team;   // [0] input tile, [1] products
+    uint32_t* tslot = (uint32_t*)(sm + TCU_OFF_BAR + 16 * TCU_TEAMS);
     const PassArgs& a = u.a;
     const TwTables<float>* tw = (const TwTables<float>*)a.tw;
-    const int t = threadIdx.x, w = t >> 5;
     int l, i, l2, k2r;
-    tcu_role_a(t, l, i);
-    tcu_role_b(u.out_kind, t, l2, k2r);
+    tcu_role_a(tt, l, i);
+    tcu_role_b(u.out_kind, tt, l2, k2r);
     const bool rowk = u.out_kind == TCU_OUT_ROW;
-    const long long G = gridDim.x;
-    unsigned char* Ah = sm + TCU_OFF_AH;
-    unsigned char* Al = sm + TCU_OFF_AL;
+    const long long G = (long long)gridDim.x * TCU_TEAMS;
+    const long long first = (long long)blockIdx.x * TCU_TEAMS + team;
+    unsigned char* Ah = stg + TCU_OFF_AH;
+    unsigned char* Al = stg + TCU_OFF_AL;
     // constants: the DFT matrix operands and the internal twiddles (with 2^-5)
     for (int q = t; q < 32 * 32; q += TCU_THREADS) {
         const int n = q >> 5, c = q & 31;
@@ -318,12 +343,12 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         const C2<float> c = tw->t[0][(ii * k1 * 16) & (TW_SIZE - 1)];
         ((float2*)(sm + TCU_OFF_TW))[k1 * 16 + ii] = make_float2(c.x, c.y);
     }
-    if (t == 0) {
+    if (tt == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tcu_smem(&bar[0])) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tcu_smem(&bar[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (w == 0) {
+    if (t < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tcu_smem(tslot)),
                      "r"(TCU_TCOLS)
                      : "memory");
@@ -334,31 +359,31 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tbase = *tslot;
-    const uint32_t d1 = tbase, d2 = tbase + 32, lane_addr = (uint32_t)(32 * w) << 16;
+    const uint32_t d1 = tbase + 64 * team, d2 = d1 + 32, lane_addr = (uint32_t)(32 * w) << 16;
     const uint32_t ah = tcu_smem(Ah), al = tcu_smem(Al), bh = tcu_smem(sm + TCU_OFF_BH), bl = tcu_smem(sm + TCU_OFF_BL);
     const float2* twt = (const float2*)(sm + TCU_OFF_TW);
     const int logNs = a.logNs;
     const float fscale = (float)a.scale;
-    bool pending = false;      // thread 0: an input copy in flight
+    bool pending = false;      // the team's issuer: an input copy in flight
     bool mma_out = false;      // products whose completion was not observed (abandoned launch)
     unsigned in_par = 0, mma_par = 0;
-    if (t == 0 && (long long)blockIdx.x < u.ntiles && !u.withhold) {
+    if (tt == 0 && first < u.ntiles && !u.withhold) {
         long long b;
         int j0;
-        tcu_tile(u, blockIdx.x, b, j0);
-        tcu_load(&imap, sm, &bar[0], j0, (int)b);
+        tcu_tile(u, first, b, j0);
+        tcu_load(&imap, stg, &bar[0], j0, (int)b);
         pending = true;
     }
-    for (long long tile = blockIdx.x; tile < u.ntiles; tile += G) {
+    for (long long tile = first; tile < u.ntiles; tile += G) {
         const bool got = tcu_wait(&bar[0], in_par, u.spin);
         // the previous tile's output store has read its staging area
-        if (t == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-        if (!__syncthreads_and(got)) {
-            if (t == 0) atomicCAS(&g_tcu_status, 0u, 1u);
+        if (tt == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        if (!tcu_team_and(team, got)) {
+            if (tt == 0) atomicCAS(&g_tcu_status, 0u, 1u);
             break;
         }
         in_par ^= 1;
-        if (t == 0) pending = false;
+        if (tt == 0) pending = false;
         long long b;
         int j0;
         tcu_tile(u, tile, b, j0);
@@ -366,7 +391,7 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         // ---- stage 1: row t = points i + 16 m of line l ----
         float2 x[16];
 #pragma unroll
-        for (int m = 0; m < 16; ++m) x[m] = *(const float2*)(sm + tcu_st_off(i + 16 * m, l));
+        for (int m = 0; m < 16; ++m) x[m] = *(const float2*)(stg + tcu_st_off(i + 16 * m, l));
         if (a.conj_in) {
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m].y = -x[m].y;
@@ -407,25 +432,25 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         const int e2 = rowk ? __shfl_sync(0xffffffffu, e1, (l2 & 1) << 3) : e1;
         if (e1 == 0) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c]);
+            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(tt, 4 * c), &x[4 * c]);
         } else {
             const float s_in = tcu_pow2(-e1);
 #pragma unroll
             for (int m = 0; m < 16; ++m) x[m] = make_float2(x[m].x * s_in, x[m].y * s_in);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(t, 4 * c), &x[4 * c]);
+            for (int c = 0; c < 4; ++c) tcu_split4(Ah, Al, tcu_a_off(tt, 4 * c), &x[4 * c]);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();   // tile read, stage-1 operand written
-        if (t == 0) {
+        tcu_team_sync(team);   // tile read, stage-1 operand written
+        if (tt == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const long long next = tile + G;
             if (next < u.ntiles) {
                 long long nb;
                 int nj0;
                 tcu_tile(u, next, nb, nj0);
-                tcu_load(&imap, sm, &bar[0], nj0, (int)nb);
+                tcu_load(&imap, stg, &bar[0], nj0, (int)nb);
                 pending = true;
             }
             tcu_mma6(d1, ah, al, bh, bl, false);
@@ -471,13 +496,13 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        if (!__syncthreads_and(ok1)) {
+        if (!tcu_team_and(team, ok1)) {
             mma_out = true;
-            if (t == 0) atomicCAS(&g_tcu_status, 0u, 2u);
+            if (tt == 0) atomicCAS(&g_tcu_status, 0u, 2u);
             break;
         }
         mma_par ^= 1;
-        if (t == 0) {
+        if (tt == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             tcu_mma6(d2, ah, al, bh, bl, true);
             tcu_commit(&bar[1]);
@@ -509,13 +534,13 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        if (!__syncthreads_and(ok2)) {
+        if (!tcu_team_and(team, ok2)) {
             mma_out = true;
-            if (t == 0) atomicCAS(&g_tcu_status, 0u, 3u);
+            if (tt == 0) atomicCAS(&g_tcu_status, 0u, 3u);
             break;
         }
         mma_par ^= 1;
-        if (t == 0) {
+        if (tt == 0) {
             if (u.out_kind == TCU_OUT_ROW) {
                 asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
                                  (uint64_t)&omap),
@@ -537,8 +562,7 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
     }
-    __syncthreads();
-    if (t == 0) {
+    if (tt == 0) {   // the team's own copies and products
         asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
         if (mma_out) tcu_wait(&bar[1], mma_par, u.spin);   // abandoned launch: products still running
         if (pending) tcu_wait(&bar[0], in_par, u.spin);    // abandoned launch: a copy still in flight
@@ -546,7 +570,7 @@ __global__ void __launch_bounds__(TCU_THREADS, TCU_MINB)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (w == 0)
+    if (t < 32)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TCU_TCOLS) : "memory");
 }
 
@@ -647,7 +671,8 @@ bool try_launch_tc_umma(const PassArgs& a, int sm_count, cudaStream_t s, bool& l
     u.withhold = withhold;
     // resident CTAs: shared memory and registers allow TCU_MINB per SM
     // (the occupancy query does not count kernels that allocate tensor memory)
-    const long long grid = std::min<long long>(u.ntiles, (long long)std::max(sm_count, 1) * TCU_MINB);
+    const long long grid = std::min<long long>((u.ntiles + TCU_TEAMS - 1) / TCU_TEAMS,
+                                               (long long)std::max(sm_count, 1) * TCU_MINB);
     if (grid <= 0) {
         launched = true;
         return true;
