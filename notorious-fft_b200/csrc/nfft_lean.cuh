@@ -158,6 +158,42 @@ struct Lean {
 #pragma unroll
                 for (int m = 0; m < 16; ++m) v[m].y = -v[m].y;
             }
+        } else if constexpr ((LOAD == LD_BLUE || LOAD == LD_FILT) && COL_IN) {
+            // first pass of a Bluestein M-point FFT: LD_C's strided addressing
+            // plus one table point per point, position p = j + (i + m R/16) Nj
+            // (forward: chirp premultiply, zero pad from N on; inverse: conj of
+            // the filter product).  All loads issued before any is used.
+            const long long rs = a.in_estride << a.logNj;
+            const C2<T>* src = (const C2<T>*)a.in + ln.bin + ln.j * a.in_estride + (long long)i * rs;
+            const long long s16 = rs << (LOGR - 4);
+            const long long p0 = ln.j + ((long long)i << a.logNj), ps = 1ll << (a.logNj + LOGR - 4);
+            const C2<T>* tab = (const C2<T>*)(LOAD == LD_BLUE ? a.chirp : a.filt) + p0;
+            // two halves of 8 points: 16 loads in flight, as for LD_C
+#pragma unroll
+            for (int hf = 0; hf < 16; hf += 8) {
+                C2<T> c[8];
+                if constexpr (LOAD == LD_BLUE) {
+#pragma unroll
+                    for (int m = hf; m < hf + 8; ++m) {
+                        const bool in = p0 + m * ps < a.N;
+                        v[m] = in ? gload(src + m * s16, a.hint_in) : mkc((T)0, (T)0);
+                        c[m - hf] = in ? gload_keep(tab + m * ps) : mkc((T)0, (T)0);
+                    }
+#pragma unroll
+                    for (int m = hf; m < hf + 8; ++m) {
+                        if (a.conj_in) v[m].y = -v[m].y;
+                        v[m] = cmul(v[m], c[m - hf]);
+                    }
+                } else {
+#pragma unroll
+                    for (int m = hf; m < hf + 8; ++m) {
+                        v[m] = gload(src + m * s16, a.hint_in);   // queue: scratch of this launch at L2
+                        c[m - hf] = gload_keep(tab + m * ps);
+                    }
+#pragma unroll
+                    for (int m = hf; m < hf + 8; ++m) v[m] = cconj(cmul(v[m], c[m - hf]));
+                }
+            }
         } else if constexpr (LOAD == LD_T4 && !COL_IN) {
             // row tile of a single-pass DCT-4 / DST-4 (line j = 0): premultiply
             // e^{-i pi p / N} of p = i + m R/16 as a chain of exact steps
@@ -358,6 +394,26 @@ struct Lean {
             } else {
 #pragma unroll
                 for (int m = 0; m < RHO; ++m) NFFT_GST(dst + m * sm_, x[m]);
+            }
+        } else if constexpr (STORE == ST_BLUE) {
+            // last pass of the inverse M-point FFT: window [0, N), back from the
+            // conjugated domain, chirp postmultiply, scale; positions q step by
+            // 2^(lns + logNso) per m.  Table loads issued before the stores.
+            constexpr int lns = lns_of<S>();
+            const long long q0 = base + ((long long)out_pos<S>(i, 0) << logNso), qs = 1ll << (lns + logNso);
+            const C2<T>* ch = (const C2<T>*)a.chirp + q0;
+            C2<T>* dst = (C2<T>*)a.out + ln.bout + q0 * a.out_estride;
+            const long long ds = qs * a.out_estride;
+            C2<T> c[RHO];
+#pragma unroll
+            for (int m = 0; m < RHO; ++m) c[m] = q0 + m * qs < a.N ? gload_keep(ch + m * qs) : mkc((T)0, (T)0);
+            const T f = (T)a.scale;
+            const T fi = a.conj_out ? -f : f;
+#pragma unroll
+            for (int m = 0; m < RHO; ++m) {
+                if (q0 + m * qs >= a.N) continue;
+                const C2<T> w = cmul(cconj(v[m]), c[m]);
+                NFFT_GST(dst + m * ds, mkc(w.x * f, w.y * fi));
             }
         } else {
 #pragma unroll
@@ -601,12 +657,25 @@ constexpr int lean_min_blocks() {
                                   : (sizeof(T) == 4 ? NFFT_LEAN_MINB_T9_F32 : 1));
 }
 
+// Tile order of a standalone Bluestein filter-product pass (LD_FILT): the
+// batch's transforms fastest, so the filter points one tile reads are read by
+// the other transforms' tiles right after it (L2 hits instead of one filter
+// sweep per transform).  A permutation of [0, tiles); identity for one
+// transform or other line layouts.
+NFFT_HD long long lean_batch_inner(const PassArgs& a, long long tile, int logJ) {
+    if (a.ndims != 2 || a.jpos != 0 || a.cnt[1] <= 1) return tile;
+    const long long tpt = a.cnt[0] >> logJ, B = a.cnt[1];
+    if ((tpt << logJ) != a.cnt[0] || tile >= tpt * B) return tile;
+    return (tile % B) * tpt + tile / B;
+}
+
 template <typename T, int LOGR, int LOGT, bool COL_IN, bool COL_OUT, int LOAD, int STORE>
 __global__ void __launch_bounds__(1 << LOGT, (lean_min_blocks<T, LOGT>()))
 lean_pass_kernel(const PassArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    lean_tile<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>(a, (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x,
-                                                           smraw);
+    long long tile = (long long)blockIdx.x + (long long)blockIdx.y * gridDim.x;
+    if constexpr (LOAD == LD_FILT) tile = lean_batch_inner(a, tile, Lean<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>::LOGJ);
+    lean_tile<T, LOGR, LOGT, COL_IN, COL_OUT, LOAD, STORE>(a, tile, smraw);
 }
 
 }  // namespace nfft

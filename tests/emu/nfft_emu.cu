@@ -896,6 +896,22 @@ bool launch_lean(const PassArgs& a, int logT, int ci, int co, int ld, int st, lo
     }
     g_launches++;
     g_lean_launches++;
+    if (ld == LD_FILT) {
+        // the kernel's tile order for the filter-product pass (lean_batch_inner):
+        // run the tiles in that order and check that it is a permutation
+        const int logJ = logT + 4 - a.logR;
+        std::vector<char> seen((size_t)ntiles, 0);
+        for (long long k = 0; k < ntiles; ++k) {
+            const long long t = lean_batch_inner(a, k, logJ);
+            if (t < 0 || t >= ntiles || seen[(size_t)t]) {
+                fprintf(stderr, "nfft_emu: filter-pass tile order is not a permutation (%lld -> %lld)\n", k, t);
+                abort();
+            }
+            seen[(size_t)t] = 1;
+            it->second(a, t, t + 1);
+        }
+        return true;
+    }
     it->second(a, 0, ntiles);
     return true;
 }
