@@ -465,9 +465,15 @@ NFFT_HD void mirror_unpack_thread(const PassArgs& a, const TwTables<T>* tw, cons
     const V ws = twiddle<T>(tw, (uint64_t)D, LOGR + 1);   // W_{2R}^D
     V ts = V{};
     if constexpr (STORE == ST_T2) ts = twiddle<T>(tw, (uint64_t)D, LOGR + 3);   // W_{8R}^D
+    // bin k = lowj + r ns is point r of the low line; bin M - k is point
+    // R - 1 - r of its partner line ns - lowj: both local lines fixed per thread
+    const int loc_lo = mirror_local(tt, ln.j, L::J, ns), loc_hi = mirror_local(tt, ns - ln.j, L::J, ns);
+    auto zrow = [&](int line, int rr) { return sm[NFFT_SM((lean_idx<true, LOGR, L::LOGJ>(line, rr)))]; };
     V wk = V{}, tk = V{};
+#pragma unroll
     for (int w = t; w < ITEMS; w += L::THREADS) {
-        const long long k = mirror_item_k(tt, l, w >> (L::LOGJ - 1), R, ns, ln.j);
+        const int r = w >> (L::LOGJ - 1);
+        const long long k = ln.j + (long long)r * ns;
         if (w == t) {
             wk = twiddle<T>(tw, (uint64_t)k, a.logN);
             if constexpr (STORE == ST_T2) tk = twiddle<T>(tw, (uint64_t)k, a.logN + 2);
@@ -475,7 +481,7 @@ NFFT_HD void mirror_unpack_thread(const PassArgs& a, const TwTables<T>* tw, cons
             wk = cmul(wk, ws);
             if constexpr (STORE == ST_T2) tk = cmul(tk, ts);
         }
-        unpack_pair_tw<T, STORE>(a, tw, ln.bout, k, M, zget, wk, tk);
+        unpack_pair_tw_z<T, STORE>(a, tw, ln.bout, k, M, zrow(loc_lo, r), zrow(loc_hi, R - 1 - r), wk, tk);
     }
 }
 

@@ -301,16 +301,20 @@ NFFT_HD void emit_bin(const PassArgs& a, const TwTables<T>* tw, long long base, 
 // Bins k and M - k (0 < k < M/2... M - 1) from their twiddles: w = W_N^k and,
 // for ST_T2, t = e^{-i pi k / 2N}.  W_N^{M-k} = -conj(W_N^k) exactly (W_N^M =
 // -1) and e^{-i pi (M-k) / 2N} = e^{-i pi / 4} conj(t): one twiddle per pair.
-template <typename T, int OP, typename Get>
-NFFT_HD void unpack_pair_tw(const PassArgs& a, const TwTables<T>* tw, long long base, long long k, long long M,
-                            Get zget, C2<T> w, C2<T> t) {
+template <typename T, int OP>
+NFFT_HD void unpack_pair_tw_z(const PassArgs& a, const TwTables<T>* tw, long long base, long long k, long long M,
+                              C2<T> zk, C2<T> zm, C2<T> w, C2<T> t) {
     using V = C2<T>;
-    V zk = zget(k), zm = zget(M - k);
     const V wm = mkc(-w.x, w.y);
     V tm = V{};
     if constexpr (OP == ST_T2) tm = mkc((t.x - t.y) * K<T>::r2, -(t.x + t.y) * K<T>::r2);
     emit_bin<T, OP>(a, tw, base, k, real_unpack<T>(zk, zm, w), t);
     emit_bin<T, OP>(a, tw, base, M - k, real_unpack<T>(zm, zk, wm), tm);
+}
+template <typename T, int OP, typename Get>
+NFFT_HD void unpack_pair_tw(const PassArgs& a, const TwTables<T>* tw, long long base, long long k, long long M,
+                            Get zget, C2<T> w, C2<T> t) {
+    unpack_pair_tw_z<T, OP>(a, tw, base, k, M, zget(k), zget(M - k), w, t);
 }
 
 // Paired unpack of one line's packed spectrum Z (M = N/2 complex values read
