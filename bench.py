@@ -1,7 +1,7 @@
 """Benchmark of the B200 FFT engine (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2c|c1|ragged|split_tc]
+                    [--workload c2c|c1|ragged|split_tc|bluestein]
 
 Workloads (synthetic, seeded; no dataset is involved):
   c2c  (default) batched complex DFT, FP64, N = 65536 x 4096 transforms per
@@ -10,6 +10,9 @@ Workloads (synthetic, seeded; no dataset is involved):
        reported beside it.  4 GiB per array > L2, so no L2 flush is needed.
   c1   256 x N=4096 FP64 dft + invdft (32 MiB per array < L2: the L2 is
        flushed by a 256 MiB write between timed steps).
+  ragged, split_tc, bluestein  profiling workloads (one ragged batch; the
+       float library's split-TC or plain form on N = 65536 x 512; FP64
+       Bluestein N = 1,000,003 x 4): time per call only.
 
 Metric: HBM GB/s of algorithmic traffic (one read + one write of every
 transform's input and output, 2 N sizeof(cmpl) bytes per transform) on the
@@ -47,6 +50,8 @@ WORKLOADS = {
     "c1": dict(N=4096, batch=256, l2="L2 flushed (256 MiB write) between steps", flush=True),
     # ragged batch in one persistent launch; `batch` = number of transforms
     "ragged": dict(N=0, batch=20000, l2="L2 flushed (256 MiB write) between steps", flush=True),
+    # profiling workload: the FP64 Bluestein case of the transform mix (prime N)
+    "bluestein": dict(N=1000003, batch=4, l2="arrays 64 MiB (no flush)", flush=False),
     # profiling workload: the float library's precision forms on N = 65536 x batch
     "split_tc": dict(N=65536, batch=512, l2="inputs 256 MiB per array > L2 (no flush)", flush=False),
 }
@@ -635,6 +640,37 @@ def run_split_tc(args, wl):
                       "gb_s": round(B * N * 16 / (ms * 1e-3) / 1e9, 1)}))
 
 
+def run_bluestein(args, wl):
+    """Profiling workload: FP64 Bluestein dft of the prime N = 1,000,003 on a
+    batch of 4 (six specialized passes over M = 2^21: chirp premultiply, two
+    plain, filter product, plain, window + chirp); prints the time per call."""
+    import torch
+
+    from notorious_fft import load
+
+    L = load(single=False)
+    stream = torch.cuda.current_stream()
+    L.set_stream(stream.cuda_stream)
+    N, B = wl["N"], wl["batch"]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(12)
+    x = torch.randn(B, N, generator=g, device="cuda", dtype=torch.complex128)
+    y = torch.empty_like(x)
+    with L.mkaux("dft", [N]) as a:
+        for _ in range(args.warmup):
+            a.batched("dft", x, y, B, N, N)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            a.batched("dft", x, y, B, N, N)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"workload": f"bluestein fp64 N={N} x{B} dft", "ms": round(ms, 4),
+                      "gb_s": round(B * N * 32 / (ms * 1e-3) / 1e9, 1)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -661,6 +697,8 @@ def main():
         return run_ragged(args, wl)
     if args.workload == "split_tc":
         return run_split_tc(args, wl)
+    if args.workload == "bluestein":
+        return run_bluestein(args, wl)
 
     import numpy as np
     import torch
