@@ -395,6 +395,23 @@ struct Lean {
 #pragma unroll
                 for (int m = 0; m < RHO; ++m) NFFT_GST(dst + m * sm_, x[m]);
             }
+        } else if constexpr (STORE == ST_C2R) {
+            // invrealdft output: each complex point is the real pair (2q, 2q+1);
+            // one vector store per point when the line's reals are pair-aligned
+            constexpr int lns = lns_of<S>();
+            const long long q0 = base + ((long long)out_pos<S>(i, 0) << logNso), qs = 1ll << (lns + logNso);
+            T* y = (T*)a.out + ln.bout;
+            const T f = (T)a.scale;
+            const T fi = a.conj_out ? -f : f;
+            if (a.out_estride == 1 && ((uintptr_t)y & (sizeof(C2<T>) - 1)) == 0) {
+                C2<T>* dst = (C2<T>*)y + q0;
+#pragma unroll
+                for (int m = 0; m < RHO; ++m) NFFT_GST(dst + m * qs, mkc(v[m].x * f, v[m].y * fi));
+            } else {
+#pragma unroll
+                for (int m = 0; m < RHO; ++m)
+                    store_elem<T, STORE>(a, tw, ln.bout, q0 + m * qs, v[m]);
+            }
         } else if constexpr (STORE == ST_BLUE) {
             // last pass of the inverse M-point FFT: window [0, N), back from the
             // conjugated domain, chirp postmultiply, scale; positions q step by
