@@ -465,7 +465,11 @@ bool run_pass(const DeviceCtx* c, const View& src, const View& dst, int logL, in
         const int ci = a.in_row ? 0 : 1, co = a.out_row ? 0 : 1;
         const bool rr = !ci && !co;
         int logT = (logR <= 12 && (rr || logR <= 10)) ? 8 : 9;
-        if (lean_logt_pref(logL) == 7 && lean_available(logR, 7, ci, co, ldop, stop)) logT = 7;
+        // 2048-point tiles where preferred, unless a column tile would keep
+        // fewer than 64 contiguous bytes per row (FP32 radix >= 2^9)
+        if (lean_logt_pref(logL) == 7 && lean_available(logR, 7, ci, co, ldop, stop) &&
+            (rr || 7 + 4 - logR >= log_jmin()))
+            logT = 7;
         if (op.logt && lean_available(logR, op.logt, ci, co, ldop, stop)) logT = op.logt;   // tuned
         if (lean_available(logR, logT, ci, co, ldop, stop)) {
             a.logJ = logT + 4 - logR;
