@@ -409,6 +409,17 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
             }
             lines[t] = LeanLine{tmp[0], tmp[1], tmp[2]};
         }
+        if constexpr (Lt::PREPACK) {
+            // the paired repack phase, then every thread's first-sub-stage reads
+            // (a barrier in the kernel) before any sub-stage write
+            for (int t = 0; t < TH; ++t) t3_prepack_thread<Lt, T>(a, tw, sm.data(), lines.data(), t);
+            std::vector<int> fl(TH), fi(TH);
+            for (int t = 0; t < TH; ++t) Lt::first_smem(a, tw, sm.data(), lines.data(), t, &regs[t * 16], fl[t], fi[t]);
+            for (int t = 0; t < TH; ++t) {
+                if constexpr (Lt::NS == 1) Lt::template write_global<0>(a, tw, lines.data(), fl[t], fi[t], &regs[t * 16]);
+                else Lt::template write_smem<0>(sm.data(), fl[t], fi[t], &regs[t * 16]);
+            }
+        } else
         for (int t = 0; t < TH; ++t) {
             int l, i;
             Lt::first(a, tw, lines.data(), t, &regs[t * 16], l, i);
