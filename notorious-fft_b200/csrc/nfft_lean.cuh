@@ -127,10 +127,10 @@ struct Lean {
     // paired stores need whole lines in the tile: row tiles, or mirror tiles
     // (column in and out) for the last pass of a multi-pass transform
     static constexpr bool MIRROR = PAIRED && COL_IN && COL_OUT;
-    // row tile of a single-pass DCT-3 / DST-3: the input repack runs as a
-    // paired phase into shared memory (t3_prepack_thread) and the first
-    // sub-stage reads its points from there
-    static constexpr bool PREPACK = LOAD == LD_T3 && !COL_IN;
+    // row tile of a single-pass DCT-3 / DST-3 or inverse real transform: the
+    // input repack runs as a paired phase into shared memory
+    // (pair_prepack_thread) and the first sub-stage reads its points from there
+    static constexpr bool PREPACK = (LOAD == LD_T3 || LOAD == LD_IR) && !COL_IN;
     static_assert(!(PAIRED && (COL_IN != COL_OUT)), "paired operators need row tiles or mirror tiles");
     static_assert(!MIRROR || LOGJ >= 1, "mirror tiles pair lines");
 
@@ -563,52 +563,70 @@ NFFT_HD void paired_unpack_thread(const PassArgs& a, const TwTables<T>* tw, cons
     }
 }
 
-// Paired DCT-3 / DST-3 input repack of a row tile (PREPACK): item (l, k),
-// k = 0 .. M/2, of the tile's lines computes zb_k and zb_{M-k} once and
-// writes the repacked points k and M - k of line l (W_N^{M-k} = -conj W_N^k
-// and e^{-i pi (M-k)/2N} = e^{-i pi/4} conj e^{-i pi k/2N} exactly), where the
-// generic operator computes both members of a pair for each point; items
-// walk k fastest so neighbouring threads read neighbouring points.
-template <typename L, typename T>
-NFFT_HD void t3_prepack_thread(const PassArgs& a, const TwTables<T>* tw, C2<T>* sm, const LeanLine* lines, int t) {
+// Paired input repack of a row tile (PREPACK): the inverse-real repack
+// p -> conj(s + i e^{+2 pi i p/N} d), s / d from the bins z_p and conj z_{M-p},
+// for invrealdft (z = the input bins; bins 1 .. M-1 halved for the adjoint of
+// realdft) and DCT-3 / DST-3 (z = the pre-twiddled reorder zb of the reals;
+// zb_0 doubled for the adjoint of DCT-2 / DST-2).  Item (l, k), k = 0 .. M/2,
+// of the tile's lines takes z_k and z_{M-k} once and writes points k and M - k
+// of line l (W_N^{M-k} = -conj W_N^k and e^{-i pi (M-k)/2N} = e^{-i pi/4}
+// conj e^{-i pi k/2N} exactly), where the generic operators compute both
+// members of a pair for each point; items walk k fastest so neighbouring
+// threads read neighbouring points.
+template <typename L, typename T, int LOAD>
+NFFT_HD void pair_prepack_thread(const PassArgs& a, const TwTables<T>* tw, C2<T>* sm, const LeanLine* lines, int t) {
     using V = C2<T>;
     constexpr int LOGR = L::LOGR_;
     constexpr int M = 1 << LOGR;
     constexpr int NI = M / 2 + 1;   // items per line
     const long long N = 2ll * M, es = a.in_estride;
+    auto rep = [](V u, V v2, V w2) {
+        const V b = cconj(v2);
+        const V s2 = cadd(u, b), d = csub(u, b);
+        const V od = cmulc(d, w2);
+        return cconj(mkc(s2.x - od.y, s2.y + od.x));
+    };
     for (int w = t; w < L::J * NI; w += L::THREADS) {
         const int l = w / NI, k = w - l * NI;
         const LeanLine ln = lines[l];
-        V* row = sm;
-        auto put = [&](int p, V val) { row[NFFT_SM((lean_idx<false, LOGR, L::LOGJ>(l, p)))] = val; };
+        auto put = [&](int p, V val) { sm[NFFT_SM((lean_idx<false, LOGR, L::LOGJ>(l, p)))] = val; };
         if (ln.j < 0) {
             put(k, mkc((T)0, (T)0));
             if (k > 0 && k < M / 2) put(M - k, mkc((T)0, (T)0));
             continue;
         }
-        const T* x = (const T*)a.in + ln.bin;
+        V zk, zm;
+        if constexpr (LOAD == LD_IR) {
+            const V* z = (const V*)a.in + ln.bin;
+            zk = NFFT_GLD(&z[k * es]);
+            zm = NFFT_GLD(&z[(M - k) * es]);
+            if (a.vjp && k > 0) {
+                zk = cscale(zk, (T)0.5);
+                zm = cscale(zm, (T)0.5);
+            }
+        } else {
+            const T* x = (const T*)a.in + ln.bin;
+            if (k == 0) {
+                zk = mkc(NFFT_GLD(&x[(a.dst ? N - 1 : 0) * es]), (T)0);
+                zm = mkc((T)K<T>::r2 * (T)2 * NFFT_GLD(&x[(a.dst ? M - 1 : M) * es]), (T)0);
+                if (a.vjp) zk = cscale(zk, (T)2);
+            } else {
+                const V tk = twiddle<T>(tw, (uint64_t)k, LOGR + 3);   // e^{-i pi k / 2N}
+                const V tm = mkc((tk.x - tk.y) * K<T>::r2, -(tk.x + tk.y) * K<T>::r2);
+                auto zb = [&](long long q, V tq) -> V {
+                    const T xr = a.dst ? NFFT_GLD(&x[(N - q - 1) * es]) : NFFT_GLD(&x[q * es]);
+                    const T xi = a.dst ? NFFT_GLD(&x[(q - 1) * es]) : NFFT_GLD(&x[(N - q) * es]);
+                    return mkc(xr * tq.x - xi * tq.y, -xr * tq.y - xi * tq.x);
+                };
+                zk = zb(k, tk);
+                zm = zb(M - k, tm);
+            }
+        }
         if (k == 0) {
-            V z0 = mkc(NFFT_GLD(&x[(a.dst ? N - 1 : 0) * es]), (T)0);
-            const V zM = mkc((T)K<T>::r2 * (T)2 * NFFT_GLD(&x[(a.dst ? M - 1 : M) * es]), (T)0);
-            if (a.vjp) z0 = cscale(z0, (T)2);
-            put(0, cconj(mkc(z0.x + zM.x, z0.x - zM.x)));
+            put(0, cconj(mkc(zk.x + zm.x, zk.x - zm.x)));
             continue;
         }
-        const V tk = twiddle<T>(tw, (uint64_t)k, LOGR + 3);   // e^{-i pi k / 2N}
-        const V tm = mkc((tk.x - tk.y) * K<T>::r2, -(tk.x + tk.y) * K<T>::r2);
-        auto zb = [&](long long q, V tq) -> V {
-            const T xr = a.dst ? NFFT_GLD(&x[(N - q - 1) * es]) : NFFT_GLD(&x[q * es]);
-            const T xi = a.dst ? NFFT_GLD(&x[(q - 1) * es]) : NFFT_GLD(&x[(N - q) * es]);
-            return mkc(xr * tq.x - xi * tq.y, -xr * tq.y - xi * tq.x);
-        };
-        const V zk = zb(k, tk), zm = zb(M - k, tm);
         const V wk = twiddle<T>(tw, (uint64_t)k, LOGR + 1);   // W_N^k
-        auto rep = [](V u, V v2, V w2) {
-            const V b = cconj(v2);
-            const V s2 = cadd(u, b), d = csub(u, b);
-            const V od = cmulc(d, w2);
-            return cconj(mkc(s2.x - od.y, s2.y + od.x));
-        };
         put(k, rep(zk, zm, wk));
         if (k < M / 2) put(M - k, rep(zm, zk, mkc(-wk.x, wk.y)));
     }
@@ -643,7 +661,7 @@ __device__ __forceinline__ void lean_tile(const PassArgs& a, long long tile, uns
     V v[16];
     int l, i;
     if constexpr (L::PREPACK) {
-        t3_prepack_thread<L, T>(a, tw, sm, lines, t);
+        pair_prepack_thread<L, T, LOAD>(a, tw, sm, lines, t);
         __syncthreads();
         L::first_smem(a, tw, sm, lines, t, v, l, i);
         __syncthreads();   // every point read before the sub-stage writes

@@ -412,7 +412,7 @@ static void emu_lean(const PassArgs& a, long long t0, long long t1) {
         if constexpr (Lt::PREPACK) {
             // the paired repack phase, then every thread's first-sub-stage reads
             // (a barrier in the kernel) before any sub-stage write
-            for (int t = 0; t < TH; ++t) t3_prepack_thread<Lt, T>(a, tw, sm.data(), lines.data(), t);
+            for (int t = 0; t < TH; ++t) pair_prepack_thread<Lt, T, LD>(a, tw, sm.data(), lines.data(), t);
             std::vector<int> fl(TH), fi(TH);
             for (int t = 0; t < TH; ++t) Lt::first_smem(a, tw, sm.data(), lines.data(), t, &regs[t * 16], fl[t], fi[t]);
             for (int t = 0; t < TH; ++t) {
